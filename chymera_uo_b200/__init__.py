@@ -1,0 +1,261 @@
+"""chymera_uo_b200 -- B200-native replacement of CHYMERA's gravitational
+potential solve (SETBDY + BDYGEN + POT3, pot/boundary.f and pot/pot3.f).
+
+The compute lives in ``libchy_pot3.so`` (CUDA, sm_100a) behind the C ABI in
+``include/chy_pot3.h``; this module is a thin ctypes layer over it.  There is
+no CPU fallback: if the library is missing, importing the solver fails.
+
+Arrays use the reference's Fortran layout: RHO and PHI are
+``(JMAX+2, KMAX+2, LMAX)`` float64 in column-major ("F") order.  Host arrays
+(numpy) are staged through the device by the library; CUDA tensors (torch)
+are used in place on the current stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libchy_pot3.so")
+
+CHY_OK = 0
+CHY_PREC_FP64 = 0
+CHY_PREC_MIXED = 1
+CHY_PTR_DEVICE = 0
+CHY_PTR_HOST = 1
+CHY_LITERAL_GCC = 0
+CHY_LITERAL_R8 = 1
+STAGES = ("forward+moments", "boundary integrals", "boundary potentials", "mode solves",
+          "inverse+ghosts+zaxphi")
+
+
+class ChyGrid(C.Structure):
+    _fields_ = [("jmax", C.c_int), ("kmax", C.c_int), ("lmax", C.c_int),
+                ("rof3n", C.c_double), ("zof3n", C.c_double),
+                ("r", C.POINTER(C.c_double)), ("z", C.POINTER(C.c_double)),
+                ("rhf", C.POINTER(C.c_double)), ("zhf", C.POINTER(C.c_double)),
+                ("pi", C.c_double), ("grav", C.c_double),
+                ("isym", C.c_int), ("maxtrm", C.c_int), ("redge", C.c_double),
+                ("npoint", C.c_int), ("literal_kind", C.c_int)]
+
+
+class ChyDiag(C.Structure):
+    _fields_ = [("tmass", C.c_double), ("phichk", C.c_double), ("klocat", C.c_int),
+                ("iterations", C.c_int), ("corr_rel", C.c_double * 8)]
+
+    def as_dict(self):
+        return {"tmass": self.tmass, "phichk": self.phichk, "klocat": self.klocat,
+                "iterations": self.iterations,
+                "corr_rel": list(self.corr_rel[: max(0, self.iterations)])}
+
+
+class ChyError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"chy status {status}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Loads libchy_pot3.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing: run `python -m chymera_uo_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, i, d, ll = C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_double, C.c_longlong
+        dpp = C.POINTER(C.c_void_p)
+        L.chy_grid_defaults.argtypes = [C.POINTER(ChyGrid), i, i, i]
+        L.chy_plan_create.argtypes = [C.POINTER(ChyGrid), i, i, C.POINTER(vp)]
+        L.chy_plan_create.restype = i
+        L.chy_plan_destroy.argtypes = [vp]
+        L.chy_solve.argtypes = [vp, vp, vp, C.POINTER(ChyDiag), i, vp]
+        L.chy_solve.restype = i
+        L.chy_solve_batch.argtypes = [vp, i, dpp, dpp, C.POINTER(ChyDiag), i, vp]
+        L.chy_solve_batch.restype = i
+        L.chy_plan_set_coef.argtypes = [vp, vp]
+        L.chy_plan_set_coef.restype = i
+        L.chy_plan_set_refine.argtypes = [vp, i]
+        L.chy_plan_set_refine.restype = i
+        L.chy_plan_device_bytes.argtypes = [vp]
+        L.chy_plan_device_bytes.restype = ll
+        L.chy_plan_bytes_per_solve.argtypes = [vp]
+        L.chy_plan_bytes_per_solve.restype = ll
+        L.chy_status_string.argtypes = [i]
+        L.chy_status_string.restype = C.c_char_p
+        L.chy_last_error.restype = C.c_char_p
+        L.chy_last_cuda_error.restype = i
+        L.chy_plan_set_profiling.argtypes = [vp, i]
+        L.chy_plan_set_profiling.restype = i
+        L.chy_plan_stage_times.argtypes = [vp, C.POINTER(C.c_double), i, C.POINTER(ll)]
+        L.chy_plan_stage_times.restype = i
+        L.chy_plan_launch_count.argtypes = [vp]
+        L.chy_plan_launch_count.restype = ll
+        L.chy_dbg_fft.argtypes = [i, i, i, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.chy_dbg_fft.restype = i
+        L.chy_dbg_realtr.argtypes = [i, i, i, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.chy_dbg_realtr.restype = i
+        L.chy_dbg_table.argtypes = [C.POINTER(ChyGrid), C.c_char_p, C.POINTER(C.c_double), ll]
+        L.chy_dbg_table.restype = ll
+        L.chy_dbg_work.argtypes = [vp, C.c_char_p, C.POINTER(C.c_double), ll]
+        L.chy_dbg_work.restype = ll
+        L.chy_dbg_umma.argtypes = [vp, i, vp, vp, i]
+        L.chy_dbg_umma.restype = i
+        _lib = L
+    return _lib
+
+
+def _check(status: int):
+    if status != CHY_OK:
+        L = lib()
+        raise ChyError(status, f"{L.chy_status_string(status).decode()}: {L.chy_last_error().decode()}")
+
+
+def grid(jmax: int, kmax: int, lmax: int, *, isym: int = 2, maxtrm: int = 10, redge: float = 0.0,
+         npoint: int = 8, literal: str = "gcc", rof3n: float | None = None,
+         zof3n: float | None = None, pi: float = 3.1415926535897932, grav: float = 1.0) -> ChyGrid:
+    """A grid descriptor with the reference's defaults (radhydro/io.f:136-140,
+    194-203; radhydro/3dhyd-main.f:166-167)."""
+    g = ChyGrid()
+    lib().chy_grid_defaults(C.byref(g), jmax, kmax, lmax)
+    g.isym, g.maxtrm, g.redge, g.npoint = isym, maxtrm, redge, npoint
+    g.literal_kind = CHY_LITERAL_R8 if literal == "r8" else CHY_LITERAL_GCC
+    if rof3n is not None:
+        g.rof3n = rof3n
+    if zof3n is not None:
+        g.zof3n = zof3n
+    g.pi, g.grav = pi, grav
+    return g
+
+
+def _is_cuda_tensor(x) -> bool:
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+class Plan:
+    """Per-grid tables + device work space for up to ``max_batch`` solves."""
+
+    def __init__(self, g: ChyGrid, precision: str = "fp64", max_batch: int = 1):
+        self.grid = g
+        self.precision = precision
+        self.shape = (g.jmax + 2, g.kmax + 2, g.lmax)
+        p = C.c_void_p()
+        prec = CHY_PREC_MIXED if precision == "mixed" else CHY_PREC_FP64
+        _check(lib().chy_plan_create(C.byref(g), prec, max_batch, C.byref(p)))
+        self._p = p
+        self.max_batch = max_batch
+
+    def close(self):
+        if getattr(self, "_p", None):
+            lib().chy_plan_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        return lib().chy_plan_device_bytes(self._p)
+
+    @property
+    def bytes_per_solve(self) -> int:
+        return lib().chy_plan_bytes_per_solve(self._p)
+
+    @property
+    def launches(self) -> int:
+        return lib().chy_plan_launch_count(self._p)
+
+    def set_refine(self, corrections: int):
+        _check(lib().chy_plan_set_refine(self._p, corrections))
+
+    def set_coef(self, coef_tensor):
+        ptr = None if coef_tensor is None else coef_tensor.data_ptr()
+        _check(lib().chy_plan_set_coef(self._p, ptr))
+
+    def set_profiling(self, on: bool):
+        _check(lib().chy_plan_set_profiling(self._p, int(on)))
+
+    def stage_times(self):
+        ms = (C.c_double * 8)()
+        calls = C.c_longlong(0)
+        n = lib().chy_plan_stage_times(self._p, ms, 8, C.byref(calls))
+        return {STAGES[i]: ms[i] for i in range(n)}, calls.value
+
+    def debug_work(self, name: str, count: int) -> np.ndarray:
+        """Copy of work array `name` of batch slot 0 (test hook)."""
+        out = np.zeros(count)
+        n = lib().chy_dbg_work(self._p, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double)), count)
+        if n < 0:
+            _check(-n)
+        return out[:n]
+
+    def _stream(self, stream):
+        if stream is not None:
+            return stream
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+
+    def solve(self, rho, phi=None, diag: bool = False, stream=None):
+        """SETBDY/BDYGEN/POT3 on one density.  numpy in -> numpy out (host
+        staging); CUDA tensor in -> CUDA tensor out (in place if phi given)."""
+        out = self.solve_batch([rho], None if phi is None else [phi], diag=diag, stream=stream)
+        return out[0] if not diag else (out[0][0], out[1][0])
+
+    def solve_batch(self, rhos, phis=None, diag: bool = False, stream=None):
+        n = len(rhos)
+        if n == 0:
+            return ([], []) if diag else []
+        dev = _is_cuda_tensor(rhos[0])
+        if phis is None:
+            if dev:
+                import torch
+                phis = [torch.zeros(self.shape[::-1], dtype=torch.float64, device=r.device).permute(2, 1, 0)
+                        for r in rhos]
+            else:
+                phis = [np.zeros(self.shape, dtype=np.float64, order="F") for _ in rhos]
+        for r, f in zip(rhos, phis):
+            self._validate(r, dev)
+            self._validate(f, dev)
+        rp = (C.c_void_p * n)(*[self._ptr(r, dev) for r in rhos])
+        fp = (C.c_void_p * n)(*[self._ptr(f, dev) for f in phis])
+        d = (ChyDiag * n)() if diag else None
+        st = self._stream(stream) if dev else (stream or 0)
+        _check(lib().chy_solve_batch(self._p, n, rp, fp, d, CHY_PTR_DEVICE if dev else CHY_PTR_HOST,
+                                     st))
+        if diag:
+            return phis, [d[i].as_dict() for i in range(n)]
+        return phis
+
+    def _validate(self, a, dev):
+        if dev:
+            if tuple(a.shape) != self.shape or a.dtype.__str__() != "torch.float64":
+                raise ValueError(f"expected float64 tensor of shape {self.shape}")
+            if a.stride() != (1, self.shape[0], self.shape[0] * self.shape[1]):
+                raise ValueError("device arrays must be column-major (Fortran) contiguous")
+        else:
+            if a.shape != self.shape or a.dtype != np.float64 or not a.flags.f_contiguous:
+                raise ValueError(f"expected Fortran-ordered float64 array of shape {self.shape}")
+
+    @staticmethod
+    def _ptr(a, dev):
+        return a.data_ptr() if dev else a.ctypes.data
+
+
+def fortran_zeros_cuda(shape, device="cuda"):
+    """A column-major float64 CUDA tensor of the given Fortran shape."""
+    import torch
+    return torch.zeros(tuple(shape[::-1]), dtype=torch.float64, device=device).permute(
+        *range(len(shape) - 1, -1, -1))
+
+
+def to_cuda_fortran(a: np.ndarray, device="cuda"):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a.T)).to(device)
+    return t.permute(*range(a.ndim - 1, -1, -1))

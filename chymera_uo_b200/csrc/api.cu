@@ -1,0 +1,438 @@
+// api.cu -- the C ABI of libchy_pot3 (include/chy_pot3.h).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "chy_pot3.h"
+#include "chy_pot3_testing.h"
+#include "planimpl.h"
+
+using namespace chy;
+
+namespace {
+
+thread_local std::string g_last_error;
+thread_local int g_last_cuda = 0;
+
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where)
+{
+    g_last_cuda = (int)e;
+    g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return CHY_ERR_CUDA;
+}
+
+#define CHY_CUDA(call)                                      \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// Packs host vectors into one device allocation (256-byte aligned pieces).
+struct Packer {
+    std::vector<char> host;
+    size_t add(const void *p, size_t bytes)
+    {
+        size_t off = (host.size() + 255) & ~(size_t)255;
+        host.resize(off + bytes);
+        if (bytes) std::memcpy(host.data() + off, p, bytes);
+        return off;
+    }
+    template <class T>
+    size_t vec(const std::vector<T> &v) { return add(v.data(), v.size() * sizeof(T)); }
+};
+
+}  // namespace
+
+extern "C" {
+
+void chy_grid_defaults(chy_grid *g, int jmax, int kmax, int lmax)
+{
+    std::memset(g, 0, sizeof(*g));
+    g->jmax = jmax;
+    g->kmax = kmax;
+    g->lmax = lmax;
+    g->rof3n = 1.0 / jmax;
+    g->zof3n = 0.5 / kmax;
+    g->pi = 3.1415926535897932;
+    g->grav = 1.0;
+    g->isym = 2;
+    g->maxtrm = 10;
+    g->redge = 0.0;
+    g->npoint = 8;
+    g->literal_kind = CHY_LITERAL_GCC;
+}
+
+const char *chy_status_string(int s)
+{
+    switch (s) {
+    case CHY_OK: return "ok";
+    case CHY_ERR_M_LT_2: return "JMAX-1 < 2 (BLKTRI IERROR=1)";
+    case CHY_ERR_N_NOT_POW2: return "KMAX-1 is not 2**k-1 (BLKTRI IERROR=2)";
+    case CHY_ERR_EIGEN: return "vertical operator eigen decomposition failed (BLKTRI IERROR=4)";
+    case CHY_ERR_IDIMY: return "leading dimension too small (BLKTRI IERROR=5)";
+    case CHY_ERR_ARG: return "invalid argument";
+    case CHY_ERR_DIMS: return "unsupported grid dimensions";
+    case CHY_ERR_UNSUPPORTED: return "unsupported ISYM/MAXTRM/NPOINT";
+    case CHY_ERR_NOT_SETUP: return "BDYGEN called before SETBDY";
+    case CHY_ERR_CUDA: return "CUDA runtime error";
+    case CHY_ERR_NOMEM: return "device allocation failed";
+    case CHY_ERR_NOCONV: return "refinement did not converge";
+    case CHY_ERR_TIMEOUT: return "a device-side bounded wait expired";
+    case CHY_ERR_CAPACITY: return "batch larger than plan capacity";
+    default: return "unknown status";
+    }
+}
+
+const char *chy_last_error(void) { return g_last_error.c_str(); }
+int chy_last_cuda_error(void) { return g_last_cuda; }
+
+void chy_plan_destroy(chy_plan *p)
+{
+    if (!p) return;
+    for (auto &e : p->ev)
+        if (e) cudaEventDestroy(e);
+    cudaFree(p->d_tables);
+    cudaFree(p->d_work);
+    cudaFree(p->stage_rho);
+    cudaFree(p->stage_phi);
+    cudaFreeHost(p->h_diag);
+    chy_mixed_release(p);
+    delete p;
+}
+
+int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **out)
+{
+    if (!g || !out || max_batch < 1) return fail(CHY_ERR_ARG, "null descriptor/output or max_batch < 1");
+    if (precision != CHY_PREC_FP64 && precision != CHY_PREC_MIXED) return fail(CHY_ERR_ARG, "unknown precision");
+    *out = nullptr;
+    chy_plan *p = new (std::nothrow) chy_plan();
+    if (!p) return fail(CHY_ERR_NOMEM, "host allocation");
+    std::string err;
+    int st = build_host_plan(*g, p->hp, err);
+    if (st != CHY_OK) {
+        delete p;
+        return fail(st, err);
+    }
+    if (precision == CHY_PREC_MIXED && !chy_mixed_supported(&p->hp)) {
+        delete p;
+        return fail(CHY_ERR_UNSUPPORTED, "mixed precision needs KMAX <= 128");
+    }
+    p->precision = precision;
+    p->max_batch = max_batch;
+    const HostPlan &hp = p->hp;
+
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (ce != cudaSuccess) {
+        delete p;
+        return cuda_fail(ce, "cudaGetDevice");
+    }
+
+    // ---- tables
+    Packer pk;
+    size_t o_twf = pk.vec(hp.fwd.twc), o_twonf = pk.vec(hp.fwd.onc), o_permf = pk.vec(hp.fwd.perm), o_rtf = pk.vec(hp.fwd.rt);
+    size_t o_twi = pk.vec(hp.inv.twc), o_twoni = pk.vec(hp.inv.onc), o_permi = pk.vec(hp.inv.perm), o_rti = pk.vec(hp.inv.rt);
+    size_t o_cosm = pk.vec(hp.cosm), o_sinm = pk.vec(hp.sinm), o_fb = pk.vec(hp.fbasis);
+    size_t o_rs = pk.vec(hp.ring_sorted), o_sring = pk.vec(hp.sring), o_sub = pk.vec(hp.sub_start);
+    size_t o_sterm = pk.vec(hp.sterm);
+    size_t o_ct = pk.vec(hp.col_term), o_cp = pk.vec(hp.col_part), o_cm_ = pk.vec(hp.col_m), o_cl = pk.vec(hp.col_l);
+    size_t o_jkj = pk.vec(hp.jk_j), o_jkk = pk.vec(hp.jk_k), o_jks = pk.vec(hp.jk_sub);
+    size_t o_bin = pk.vec(hp.jk_bin), o_hout = pk.vec(hp.jk_hout);
+    size_t o_am = pk.vec(hp.am), o_cmv = pk.vec(hp.cm), o_cc = pk.vec(hp.cc), o_bm0 = pk.vec(hp.bm0), o_xl = pk.vec(hp.xlamm);
+    size_t o_an = pk.vec(hp.an), o_bn = pk.vec(hp.bn), o_cn = pk.vec(hp.cn);
+    size_t o_U = pk.vec(hp.U), o_V = pk.vec(hp.V), o_lam = pk.vec(hp.lam);
+    size_t o_ext = chy_mixed_pack_tables(&hp, &pk.host);
+    p->table_bytes = pk.host.size();
+    ce = cudaMalloc(&p->d_tables, p->table_bytes);
+    if (ce == cudaSuccess) ce = cudaMemcpy(p->d_tables, pk.host.data(), p->table_bytes, cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) {
+        chy_plan_destroy(p);
+        return ce == cudaErrorMemoryAllocation ? fail(CHY_ERR_NOMEM, "tables") : cuda_fail(ce, "tables");
+    }
+    char *D = p->d_tables;
+    DevTables &t = p->t;
+    t.J = hp.J; t.K = hp.K; t.L = hp.L; t.N = hp.N; t.M = hp.M; t.NZ = hp.NZ;
+    t.nring = hp.nring; t.nkeep = hp.nkeep; t.njk = hp.njk; t.ncol = hp.ncol;
+    t.nsub = (int)hp.sub_start.size() - 1; t.ntrm = hp.ntrm; t.maxtrm = g->maxtrm;
+    t.isyma = g->isym < 0 ? -g->isym : g->isym; t.npoint = hp.npoint;
+    t.sf1 = hp.sf1; t.pig4 = hp.pig4; t.grav = g->grav;
+    t.F1 = (t.isyma == 1) ? 1.0 : 0.0;
+    t.cmmax = hp.cmmax; t.ammin = hp.ammin; t.cnmax = hp.cnmax;
+    auto setfft = [&](FftDev &f, const FftSchedule &s, size_t otw, size_t oon, size_t operm, size_t ort) {
+        f.n = s.n; f.isn = s.isn; f.nst = s.nstage; f.nh = s.nh; f.ncompact = s.ncompact;
+        for (int i = 0; i < s.nstage; i++) { f.radix[i] = s.radix[i]; f.span[i] = s.span[i]; f.off[i] = s.off[i]; }
+        f.twc = (const double *)(D + otw); f.onc = (const uint8_t *)(D + oon);
+        f.perm = (const int *)(D + operm); f.rt = (const double *)(D + ort);
+    };
+    setfft(t.fwd, hp.fwd, o_twf, o_twonf, o_permf, o_rtf);
+    setfft(t.inv, hp.inv, o_twi, o_twoni, o_permi, o_rti);
+    if (!fft_shape_supported(t.fwd, hp.L) || !fft_shape_supported(t.inv, hp.L)) {
+        chy_plan_destroy(p);
+        return fail(CHY_ERR_DIMS, "no device transform for this LMAX");
+    }
+    t.cosm = (const double *)(D + o_cosm); t.sinm = (const double *)(D + o_sinm);
+    t.fbasis = (const double *)(D + o_fb);
+    t.ring_sorted = (const int *)(D + o_rs); t.sring = (const double *)(D + o_sring);
+    t.sterm = (const double *)(D + o_sterm); t.srow = hp.srow;
+    t.sub_start = (const int *)(D + o_sub);
+    t.col_term = (const int *)(D + o_ct); t.col_part = (const int *)(D + o_cp);
+    t.col_m = (const int *)(D + o_cm_); t.col_l = (const int *)(D + o_cl);
+    t.jk_j = (const int *)(D + o_jkj); t.jk_k = (const int *)(D + o_jkk); t.jk_sub = (const int *)(D + o_jks);
+    t.jk_bin = (const double *)(D + o_bin); t.jk_hout = (const double *)(D + o_hout);
+    t.am = (const double *)(D + o_am); t.cm = (const double *)(D + o_cmv); t.cc = (const double *)(D + o_cc);
+    t.bm0 = (const double *)(D + o_bm0); t.xlamm = (const double *)(D + o_xl);
+    t.an = (const double *)(D + o_an); t.bn = (const double *)(D + o_bn); t.cn = (const double *)(D + o_cn);
+    t.U = (const double *)(D + o_U); t.V = (const double *)(D + o_V); t.lam = (const double *)(D + o_lam);
+    for (int i = 0; i < 11; i++) t.zx[i] = hp.zx[i];
+    chy_mixed_bind_tables(p, D + o_ext);
+
+    // ---- work space
+    const size_t nX = (size_t)hp.L * hp.K * hp.J;
+    const size_t nsub = hp.sub_start.size() - 1;
+    Work &w = p->w;
+    w.sX = nX;
+    w.sW = precision == CHY_PREC_FP64 ? nX : 0;
+    w.sC = precision == CHY_PREC_FP64 ? nX : 0;
+    w.smom = (size_t)21 * hp.nring;
+    w.ssub = nsub * 2 * hp.ncol;
+    w.sscan = (nsub + 1) * 2 * hp.ncol;
+    w.sphac = (size_t)hp.K + 2;
+    w.sdiag = 4;
+    size_t per = w.sX + w.sW + w.sC + w.smom + w.ssub + w.sscan + w.sphac + w.sdiag;
+    size_t ext = chy_mixed_work_doubles(p);
+    p->work_bytes = (per * max_batch + ext) * sizeof(double) + 4096;
+    ce = cudaMalloc(&p->d_work, p->work_bytes);
+    if (ce != cudaSuccess) {
+        chy_plan_destroy(p);
+        return fail(CHY_ERR_NOMEM, "work space");
+    }
+    double *q = (double *)p->d_work;
+    w.X = q; q += w.sX * max_batch;
+    w.W = q; q += w.sW * max_batch;
+    w.C = q; q += w.sC * max_batch;
+    w.mom = q; q += w.smom * max_batch;
+    w.sub = q; q += w.ssub * max_batch;
+    w.scan = q; q += w.sscan * max_batch;
+    w.phac = q; q += w.sphac * max_batch;
+    w.diag = q; q += w.sdiag * max_batch;
+    w.coef = nullptr;
+    chy_mixed_bind_work(p, q);
+    CHY_CUDA(cudaMemset(p->d_work, 0, p->work_bytes));
+    p->nvol = (size_t)(hp.J + 2) * (hp.K + 2) * hp.L;
+    CHY_CUDA(cudaMallocHost(&p->h_diag, sizeof(double) * 4 * max_batch));
+    for (auto &e : p->ev) CHY_CUDA(cudaEventCreate(&e));
+    *out = p;
+    return CHY_OK;
+}
+
+int chy_plan_set_coef(chy_plan *p, double *coef_dev)
+{
+    if (!p) return fail(CHY_ERR_ARG, "null plan");
+    p->w.coef = coef_dev;
+    return CHY_OK;
+}
+
+int chy_plan_set_refine(chy_plan *p, int corrections)
+{
+    if (!p || corrections < 0 || corrections > 8) return fail(CHY_ERR_ARG, "corrections must be 0..8");
+    p->refine = corrections;
+    return CHY_OK;
+}
+
+long long chy_plan_device_bytes(const chy_plan *p)
+{
+    if (!p) return 0;
+    return (long long)(p->table_bytes + p->work_bytes);
+}
+
+long long chy_plan_bytes_per_solve(const chy_plan *p)
+{
+    if (!p) return 0;
+    const Work &w = p->w;
+    size_t per = w.sX + w.sW + w.sC + w.smom + w.ssub + w.sscan + w.sphac + w.sdiag;
+    return (long long)(per * sizeof(double));
+}
+
+int chy_plan_set_profiling(chy_plan *p, int on)
+{
+    if (!p) return fail(CHY_ERR_ARG, "null plan");
+    p->profile = on != 0;
+    for (double &v : p->stage_ms) v = 0.0;
+    p->stage_calls = 0;
+    return CHY_OK;
+}
+
+int chy_plan_stage_times(const chy_plan *p, double *ms, int n, long long *calls)
+{
+    if (!p || !ms) return fail(CHY_ERR_ARG, "null argument");
+    for (int i = 0; i < n && i < ST_NSTAGE; i++) ms[i] = p->stage_ms[i];
+    if (calls) *calls = p->stage_calls;
+    return ST_NSTAGE;
+}
+
+long long chy_plan_launch_count(const chy_plan *p) { return p ? p->launches : 0; }
+
+}  // extern "C"
+
+// One launch sequence over nb solves whose caller buffers are in bp.
+static int run_batch(chy_plan *p, const BatchPtrs &bp, int nb, cudaStream_t s)
+{
+    const DevTables &t = p->t;
+    const bool prof = p->profile;
+    auto mark = [&](int i) -> cudaError_t { return prof ? cudaEventRecord(p->ev[i], s) : cudaSuccess; };
+    CHY_CUDA(mark(0));
+    CHY_CUDA(launch_forward(t, bp, p->w, nb, s));
+    CHY_CUDA(mark(1));
+    CHY_CUDA(launch_bdy_sums(t, p->w, nb, s));
+    CHY_CUDA(mark(2));
+    CHY_CUDA(launch_bdy_synth(t, p->w, nb, s));
+    CHY_CUDA(mark(3));
+    int nl = 0;
+    if (p->precision == CHY_PREC_FP64) {
+        CHY_CUDA(launch_solve_fp64(t, p->w, nb, p->num_sms, s));
+        nl = 3;
+    } else {
+        int st = chy_mixed_solve(p, nb, s, &nl);
+        if (st != CHY_OK) return st;
+    }
+    CHY_CUDA(mark(4));
+    CHY_CUDA(launch_inverse(t, bp, p->w, nb, s));
+    CHY_CUDA(mark(5));
+    p->launches += 1 + 2 + 1 + nl + 2;
+    if (prof) {
+        CHY_CUDA(cudaEventSynchronize(p->ev[ST_NSTAGE]));
+        for (int i = 0; i < ST_NSTAGE; i++) {
+            float ms = 0.f;
+            CHY_CUDA(cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]));
+            p->stage_ms[i] += ms;
+        }
+        p->stage_calls++;
+    }
+    return CHY_OK;
+}
+
+static int fetch_diag(chy_plan *p, chy_diag *diag, int nb, int first, cudaStream_t s)
+{
+    if (!diag) return CHY_OK;
+    CHY_CUDA(cudaMemcpyAsync(p->h_diag, p->w.diag, sizeof(double) * 4 * nb, cudaMemcpyDeviceToHost, s));
+    CHY_CUDA(cudaStreamSynchronize(s));
+    const int st = chy_mixed_collect(p, nb);
+    if (st != CHY_OK) return fail(st, st == CHY_ERR_TIMEOUT ? "mode solve: bounded wait expired" : "mode solve readback");
+    for (int i = 0; i < nb; i++) {
+        chy_diag &d = diag[first + i];
+        d.tmass = p->h_diag[4 * i + 0];
+        d.phichk = p->h_diag[4 * i + 1];
+        d.klocat = (int)p->h_diag[4 * i + 2];
+        chy_mixed_fill_diag(p, i, &d);
+    }
+    return CHY_OK;
+}
+
+extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, double *const *phi,
+                               chy_diag *diag, int ptr_kind, void *stream)
+{
+    if (!p || n < 0 || (n > 0 && (!rho || !phi))) return fail(CHY_ERR_ARG, "null plan or buffers");
+    cudaStream_t s = (cudaStream_t)stream;
+    const HostPlan &hp = p->hp;
+    const size_t J2 = hp.J + 2, K2 = hp.K + 2, L = hp.L, bytes = p->nvol * sizeof(double);
+    for (int i = 0; i < n; i++)
+        if (!rho[i] || !phi[i]) return fail(CHY_ERR_ARG, "null rho/phi pointer");
+    if (ptr_kind == CHY_PTR_DEVICE) {
+        for (int first = 0; first < n;) {
+            const int nb = std::min(std::min(n - first, p->max_batch), kMaxBatchPtrs);
+            BatchPtrs bp{};
+            for (int i = 0; i < nb; i++) { bp.rho[i] = rho[first + i]; bp.phi[i] = phi[first + i]; }
+            int st = run_batch(p, bp, nb, s);
+            if (st != CHY_OK) return st;
+            st = fetch_diag(p, diag, nb, first, s);
+            if (st != CHY_OK) return st;
+            first += nb;
+        }
+        return CHY_OK;
+    }
+    if (ptr_kind != CHY_PTR_HOST) return fail(CHY_ERR_ARG, "ptr_kind");
+    // host buffers: stage through device copies, one solve at a time
+    if (!p->stage_rho) {
+        CHY_CUDA(cudaMalloc(&p->stage_rho, bytes));
+        CHY_CUDA(cudaMalloc(&p->stage_phi, bytes));
+    }
+    for (int i = 0; i < n; i++) {
+        CHY_CUDA(cudaMemcpyAsync(p->stage_rho, rho[i], bytes, cudaMemcpyHostToDevice, s));
+        // cells the solve never writes keep the caller's values:
+        // PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :)
+        CHY_CUDA(cudaMemcpy2DAsync(p->stage_phi + J2 * (K2 - 1), J2 * K2 * sizeof(double),
+                                   phi[i] + J2 * (K2 - 1), J2 * K2 * sizeof(double), J2 * sizeof(double),
+                                   L, cudaMemcpyHostToDevice, s));
+        CHY_CUDA(cudaMemcpy2DAsync(p->stage_phi + (J2 - 1), J2 * K2 * sizeof(double), phi[i] + (J2 - 1),
+                                   J2 * K2 * sizeof(double), sizeof(double), L, cudaMemcpyHostToDevice, s));
+        BatchPtrs bp{};
+        bp.rho[0] = p->stage_rho;
+        bp.phi[0] = p->stage_phi;
+        int st = run_batch(p, bp, 1, s);
+        if (st != CHY_OK) return st;
+        CHY_CUDA(cudaMemcpyAsync(phi[i], p->stage_phi, bytes, cudaMemcpyDeviceToHost, s));
+        st = fetch_diag(p, diag, 1, i, s);
+        if (st != CHY_OK) return st;
+    }
+    CHY_CUDA(cudaStreamSynchronize(s));
+    return CHY_OK;
+}
+
+extern "C" int chy_solve(chy_plan *p, const double *rho, double *phi, chy_diag *diag, int ptr_kind,
+                         void *stream)
+{
+    const double *r[1] = {rho};
+    double *f[1] = {phi};
+    return chy_solve_batch(p, 1, r, f, diag, ptr_kind, stream);
+}
+
+// Test hook: copies a work array of batch slot 0 to the host (synchronous).
+extern "C" long long chy_dbg_work(chy_plan *p, const char *name, double *out, long long cap)
+{
+    if (!p || !name || !out) return -CHY_ERR_ARG;
+    const std::string n(name);
+    const double *src = nullptr;
+    size_t cnt = 0;
+    if (n == "X") { src = p->w.X; cnt = p->w.sX; }
+    else if (n == "mom") { src = p->w.mom; cnt = p->w.smom; }
+    else if (n == "sub") { src = p->w.sub; cnt = p->w.ssub; }
+    else if (n == "scan") { src = p->w.scan; cnt = p->w.sscan; }
+    else if (n == "phac") { src = p->w.phac; cnt = p->w.sphac; }
+    else if (n == "diag") { src = p->w.diag; cnt = p->w.sdiag; }
+    else return -CHY_ERR_ARG;
+    if ((long long)cnt > cap) cnt = (size_t)cap;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(out, src, cnt * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return -cuda_fail(e, "chy_dbg_work");
+    return (long long)cnt;
+}
+
+#include <mutex>
+#include <unordered_map>
+
+cudaError_t chy::ensure_smem(const void *kernel, size_t bytes)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void *, int> done[64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    auto &m = done[dev & 63];
+    auto it = m.find(kernel);
+    if (it != m.end() && it->second >= (int)bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) m[kernel] = (int)bytes;
+    return e;
+}

@@ -1,0 +1,70 @@
+// dbg.cpp -- host-only test hooks (include/chy_pot3_testing.h).
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "chy_pot3_testing.h"
+#include "plan.h"
+
+using namespace chy;
+
+extern "C" int chy_dbg_fft(int n, int isn, int literal_kind, double *a, double *b)
+{
+    FftSchedule s;
+    int st = build_fft_schedule(n, isn, literal_kind == CHY_LITERAL_R8, s);
+    if (st != CHY_OK) return st;
+    fft_apply_host(s, a, b);
+    return CHY_OK;
+}
+
+extern "C" int chy_dbg_realtr(int n, int isn, int literal_kind, double *a, double *b)
+{
+    FftSchedule s;
+    int st = build_fft_schedule(n, isn, literal_kind == CHY_LITERAL_R8, s);
+    if (st != CHY_OK) return st;
+    realtr_apply_host(s, a, b);
+    return CHY_OK;
+}
+
+template <class T>
+static long long put(const std::vector<T> &v, double *out, long long cap)
+{
+    long long n = (long long)v.size();
+    for (long long i = 0; i < n && i < cap; i++) out[i] = (double)v[i];
+    return n;
+}
+
+extern "C" long long chy_dbg_table(const chy_grid *g, const char *name, double *out, long long cap)
+{
+    if (!g || !name || !out) return -CHY_ERR_ARG;
+    HostPlan hp;
+    std::string err;
+    int st = build_host_plan(*g, hp, err);
+    if (st != CHY_OK) return -st;
+    const std::string n(name);
+    if (n == "U") return put(hp.U, out, cap);
+    if (n == "V") return put(hp.V, out, cap);
+    if (n == "lam") return put(hp.lam, out, cap);
+    if (n == "an") return put(hp.an, out, cap);
+    if (n == "bn") return put(hp.bn, out, cap);
+    if (n == "cn") return put(hp.cn, out, cap);
+    if (n == "am") return put(hp.am, out, cap);
+    if (n == "cm") return put(hp.cm, out, cap);
+    if (n == "cc") return put(hp.cc, out, cap);
+    if (n == "bm0") return put(hp.bm0, out, cap);
+    if (n == "xlamm") return put(hp.xlamm, out, cap);
+    if (n == "ring_term") return put(hp.ring_term, out, cap);
+    if (n == "ring_dv") return put(hp.ring_dv, out, cap);
+    if (n == "ring_rsph") return put(hp.ring_rsph, out, cap);
+    if (n == "jk_split") return put(hp.jk_split, out, cap);
+    if (n == "jk_bin") return put(hp.jk_bin, out, cap);
+    if (n == "jk_hout") return put(hp.jk_hout, out, cap);
+    if (n == "sub_start") return put(hp.sub_start, out, cap);
+    if (n == "jk_sub") return put(hp.jk_sub, out, cap);
+    if (n == "scalars") {
+        std::vector<double> v = {hp.sf1, hp.pig4, hp.cmmax, hp.ammin, hp.cnmax, (double)hp.nkeep,
+                                 (double)hp.ncol, (double)(hp.sub_start.size() - 1)};
+        return put(v, out, cap);
+    }
+    return -CHY_ERR_ARG;
+}

@@ -1,0 +1,88 @@
+// devplan.h -- device-resident tables of one grid and the launch interface of
+// the kernels (internal to libchy_pot3).
+//
+// HBM layout of one solve's work space:
+//   X    [L][K][J]   FP64  azimuthal mode coefficients.  X[l][k][j] is mode l of
+//                          PHI(J=j+2, K=k+2): j < J-1, k < K-1 is the interior
+//                          (the unknowns of the mode solve), j = J-1 the outer
+//                          boundary column, k = K-1 the top boundary row.
+//   W    [L][J][K]   FP64  vertical eigen coefficients of the mode solve
+//   C    [L][J][K]   FP64  radial elimination multipliers (FP64 solve path)
+//   MOM  [21][nring] FP64  per-ring azimuthal moments sum_l {1, cos m psi_l,
+//                          sin m psi_l} rho, ring = k*(J-1) + j.
+//   SUB  [nsub][2][ncol]   per sub-chunk sums of the boundary integrands.
+//   SCAN [nsub+1][2][ncol] exclusive prefix (inside) / suffix (outside) sums.
+//   PHAC [K+2]             ZAXPHI deviations; DIAG [4] TMASS, PHICHK, KLOCAT.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace chy {
+
+constexpr int kMaxStage = 16;
+constexpr int kMaxBatchPtrs = 64;   // caller pointers passed per launch
+constexpr int kSubChunk = 64;       // rings per boundary sub-chunk
+
+struct FftDev {
+    int n, isn, nst, nh, ncompact;
+    int radix[kMaxStage], span[kMaxStage], off[kMaxStage];
+    const double *twc;     // [ncompact][6] rotation of position j of stage s at off[s]+j
+    const uint8_t *onc;    // [ncompact]
+    const int *perm;       // [n]
+    const double *rt;      // [nh][2]
+};
+
+// True when the device kernels' compile-time stage structure for this LMAX
+// equals the recorded schedule.
+bool fft_shape_supported(const FftDev &f, int L);
+
+struct DevTables {
+    int J, K, L, N, M, NZ, nring, nkeep, njk, ncol, nsub, ntrm, maxtrm, isyma, npoint;
+    double sf1, pig4, grav, F1, cmmax, ammin, cnmax;
+    FftDev fwd, inv;
+    const double *cosm, *sinm;      // [10][L]
+    const double *fbasis;           // [21][L] transforms of {1, cos m psi, sin m psi}
+    // kept rings in ascending spherical radius: ring index, and rsph, C1, S1, DV
+    const int *ring_sorted;
+    const double *sring;            // [nkeep][4]
+    const double *sterm;            // [nkeep][srow]: TERM(1..NTRM), r^-(2l+1) l=0..10, DV
+    int srow;
+    const int *sub_start;           // [nsub+1] sub-chunk boundaries in sorted order
+    const int *col_term, *col_part, *col_m, *col_l;   // [ncol]
+    const int *jk_j, *jk_k, *jk_sub;                  // [njk]; jk_sub = first sub-chunk outside
+    const double *jk_bin, *jk_hout;                   // [njk][66]
+    // stencil (radial length M, vertical length NZ)
+    const double *am, *cm, *cc, *bm0, *xlamm, *an, *bn, *cn;
+    // vertical eigenbasis, row-major [NZ][NZ]: U(p,k) and V(k,p)
+    const double *U, *V, *lam;
+    double zx[11];
+};
+
+// Per-launch batch addressing.  Caller arrays come as pointer lists; the
+// library's work arrays are one allocation with a fixed per-solve stride.
+struct BatchPtrs {
+    const double *rho[kMaxBatchPtrs];
+    double *phi[kMaxBatchPtrs];
+};
+
+struct Work {
+    double *X, *W, *C, *mom, *sub, *scan, *phac, *diag;
+    size_t sX, sW, sC, smom, ssub, sscan, sphac, sdiag;   // per-solve strides (elements)
+    double *coef;                                    // optional /COEFS/ output (solve 0 only)
+};
+
+// Raises a kernel's dynamic shared-memory limit on the current device the
+// first time a launch needs it; the attribute persists, so later launches make
+// no runtime call (a per-launch cudaFuncSetAttribute stalls the issue stream).
+cudaError_t ensure_smem(const void *kernel, size_t bytes);
+
+// kernels (k_fft.cu, k_bdy.cu, k_solve.cu)
+cudaError_t launch_forward(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s);
+cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStream_t s);
+cudaError_t launch_bdy_synth(const DevTables &t, const Work &w, int nb, cudaStream_t s);
+cudaError_t launch_solve_fp64(const DevTables &t, const Work &w, int nb, int num_sms, cudaStream_t s);
+cudaError_t launch_inverse(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s);
+
+}  // namespace chy

@@ -1,0 +1,122 @@
+// k_bdy.cu -- BDYGEN's mass integrals without the O(rings x boundary points)
+// masked accumulation.
+//
+// The reference adds every ring's multipole contribution MRING into
+// MASSIN(JK) for each boundary point JK with RSPHER <= RBDY(JK), and its
+// r^-(2l+1)-scaled contribution into MASSOUT(JK) for RSPHER > RBDY(JK)
+// (pot/boundary.f:558-604): ~1.6 G adds at 256x128.  With the rings sorted by
+// spherical radius, MASSIN(JK) is a prefix sum and MASSOUT(JK) a suffix sum
+// of the same sequence, cut at the number of rings inside RBDY(JK).  The
+// sorted sequence is split into sub-chunks that never straddle a cut; one CTA
+// sums each sub-chunk, one thread per column scans the sub-chunk sums.  Every
+// sum has a fixed order, so results are bit-reproducible alone or in a batch.
+// The outside sums are accumulated from the outermost ring inward, so the
+// huge r^-(2l+1) factors of inner rings never enter a difference.
+//
+// Compiled with --fmad=false so the ring terms equal the host tables bitwise.
+#include "devplan.h"
+#include "legendre.h"
+
+namespace chy {
+
+__constant__ LegTerm c_leg[66] = CHY_LEG_TABLE;
+
+// Grid: (nsub, 1, batch), 256 threads.
+__global__ void __launch_bounds__(256) k_bdy_sub(DevTables t, Work w)
+{
+    extern __shared__ double smem[];
+    const int RL = t.srow, NT_ = t.ntrm;
+    double *s_row = smem;                                      // [ns][RL]: TERM, r^-(2l+1), DV
+    double (*s_mom)[21] = reinterpret_cast<double (*)[21]>(smem + kSubChunk * RL);
+    const int sc = blockIdx.x, b = blockIdx.z;
+    const int s0 = t.sub_start[sc], s1 = t.sub_start[sc + 1], ns = s1 - s0;
+    const double *mom = w.mom + (size_t)b * w.smom;
+
+    // per ring, geometry from the plan (TERM(I) of pot/boundary.f:385-502,
+    // r^-(2l+1) of :587, DV of :516) and DV * moments from this solve
+    for (int i = threadIdx.x; i < ns * RL; i += blockDim.x) s_row[i] = t.sterm[(size_t)s0 * RL + i];
+    __syncthreads();
+    for (int it = threadIdx.x; it < ns * 21; it += blockDim.x) {
+        const int r = it / 21, q = it % 21;
+        s_mom[r][q] = s_row[r * RL + NT_ + 11] * mom[(size_t)q * t.nring + t.ring_sorted[s0 + r]];
+    }
+    __syncthreads();
+
+    double *sub = w.sub + (size_t)b * w.ssub + (size_t)sc * 2 * t.ncol;
+    for (int cc = threadIdx.x; cc < 2 * t.ncol; cc += blockDim.x) {
+        const int col = cc % t.ncol, out = cc / t.ncol;
+        const int term = t.col_term[col], m = t.col_m[col], l = t.col_l[col];
+        const int mq = t.col_part[col] == 0 ? m : 10 + m;
+        double acc = 0.0;
+        if (!out) {
+            for (int r = 0; r < ns; ++r) acc = acc + s_row[r * RL + term] * s_mom[r][mq];
+        } else {
+            for (int r = 0; r < ns; ++r) acc = acc + (s_row[r * RL + term] * s_mom[r][mq]) * s_row[r * RL + NT_ + l];
+        }
+        sub[(size_t)out * t.ncol + col] = acc;
+    }
+}
+
+// Grid: (2*ncol, 1, batch), 256 threads: one CTA scans one column.
+// scan[i][0][col] = sum of inside sums of sub-chunks < i (prefix from the
+// innermost ring); scan[i][1][col] = sum of outside sums of sub-chunks >= i
+// (suffix from the outermost ring).  Each thread owns a contiguous run of
+// sub-chunks; runs are combined by a fixed-shape block scan, so the result is
+// bit-reproducible.
+__global__ void __launch_bounds__(256) k_bdy_scan(DevTables t, Work w)
+{
+    __shared__ double warp_tot[8];
+    const int cc = blockIdx.x, b = blockIdx.z;
+    const int col = cc % t.ncol, out = cc / t.ncol;
+    const double *__restrict__ sub = w.sub + (size_t)b * w.ssub;
+    double *__restrict__ scan = w.scan + (size_t)b * w.sscan;
+    const size_t ld = (size_t)2 * t.ncol, off = (size_t)out * t.ncol + col;
+    const int ns = t.nsub, per = (ns + 255) / 256;
+    const int lo = threadIdx.x * per, hi = min(lo + per, ns);
+    // position p in scan order -> sub-chunk index
+    auto idx = [&](int p) { return out ? ns - 1 - p : p; };
+    double local = 0.0;
+    for (int p = lo; p < hi; ++p) local = local + sub[(size_t)idx(p) * ld + off];
+    // exclusive block scan of the per-thread totals
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double incl = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        const double v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl = incl + v;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    double base = 0.0;
+    for (int i = 0; i < wid; ++i) base = base + warp_tot[i];
+    double run = base + (incl - local);
+    for (int p = lo; p < hi; ++p) {
+        const int i = idx(p);
+        const double v = sub[(size_t)i * ld + off];
+        if (!out) {
+            scan[(size_t)i * ld + off] = run;
+            run = run + v;
+        } else {
+            run = run + v;
+            scan[(size_t)i * ld + off] = run;
+        }
+    }
+    if (threadIdx.x == 255) {
+        double tot = 0.0;
+        for (int i = 0; i < 8; ++i) tot = tot + warp_tot[i];
+        scan[(size_t)ns * ld + off] = out ? 0.0 : tot;
+    }
+}
+
+cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStream_t s)
+{
+    const size_t sm = (size_t)kSubChunk * (t.srow + 21) * sizeof(double);
+    cudaError_t e = ensure_smem((const void *)k_bdy_sub, sm);
+    if (e != cudaSuccess) return e;
+    k_bdy_sub<<<dim3(t.nsub, 1, nb), 256, sm, s>>>(t, w);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_bdy_scan<<<dim3(2 * t.ncol, 1, nb), 256, 0, s>>>(t, w);
+    return cudaGetLastError();
+}
+
+}  // namespace chy

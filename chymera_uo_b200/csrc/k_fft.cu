@@ -1,0 +1,605 @@
+// k_fft.cu -- azimuthal transforms and everything fused with them.
+//
+// Compiled with --fmad=false: every product and sum of the transforms is a
+// separately rounded IEEE operation, in the order pot/fft.f performs it, so
+// the device transform reproduces the reference's (single-precision-angle)
+// transform bit for bit.  Fused multiply-adds are requested explicitly
+// (__fma_rn) only where the reference order is not reproduced anyway (ring
+// moments, boundary synthesis).
+//
+// One CTA owns TC adjacent (J,K) columns and holds their LMAX samples in
+// shared memory as rows of stride RS = TC+1 doubles: row 2q is Re(z_q) and
+// row 2q+1 is Im(z_q) of the LMAX/2-point complex sequence
+// z_q = rho(2q) + i rho(2q+1) that POT3 builds (pot/pot3.f:95-98).  Global
+// loads and stores run along J, the fastest dimension of the reference's
+// arrays, so they are coalesced.  The stage structure is fixed at compile time
+// per LMAX; the rotations, output permutation and REALTR recurrence values are
+// the recorded tables, staged in shared memory.
+#include "devplan.h"
+
+namespace chy {
+
+// ---------------------------------------------------------------------------
+// Compile-time stage structure of pot/fft.f's factorisation for N = 2^e
+// (fft.f:147-187): [4]^a, middle, [4]^a with e = 4a + r and middle = {},
+// {2}, {4}, {2,2,2} for r = 0..3.
+// ---------------------------------------------------------------------------
+template <int N>
+struct Shape {
+    static constexpr int log2n()
+    {
+        int e = 0;
+        while ((1 << e) < N) ++e;
+        return e;
+    }
+    static constexpr int nst()
+    {
+        const int e = log2n(), a = e / 4, r = e % 4;
+        return 2 * a + (r == 0 ? 0 : (r == 3 ? 3 : 1));
+    }
+    static constexpr int radix(int s)
+    {
+        const int e = log2n(), a = e / 4, r = e % 4;
+        if (s < a || s >= nst() - a) return 4;
+        return r == 2 ? 4 : 2;
+    }
+    static constexpr int span(int s)
+    {
+        int sp = N;
+        for (int i = 0; i <= s; ++i) sp /= radix(i);
+        return sp;
+    }
+};
+
+template <int L>
+struct Tile {
+    static constexpr int N = L / 2;
+    static constexpr int TC = L <= 128 ? 32 : (L <= 256 ? 16 : 8);  // columns per CTA
+    static constexpr int RS = TC + 1;                               // row stride (doubles)
+    static constexpr int ROWS = L + 2;
+    static constexpr int TPC = 256 / TC;                            // threads per column
+};
+
+// Shared-memory copy of one direction's tables.
+struct FftSmem {
+    double *tw;        // [ncompact][6]
+    uint8_t *on;       // [ncompact]
+    int *perm;         // [n]
+    double *rt;        // [nh][2]
+};
+
+__device__ __forceinline__ void load_fft_tables(const FftDev &f, const FftSmem &s)
+{
+    for (int i = threadIdx.x; i < f.ncompact * 6; i += blockDim.x) s.tw[i] = f.twc[i];
+    for (int i = threadIdx.x; i < f.ncompact; i += blockDim.x) s.on[i] = f.onc[i];
+    for (int i = threadIdx.x; i < f.n; i += blockDim.x) s.perm[i] = f.perm[i];
+    for (int i = threadIdx.x; i < 2 * f.nh; i += blockDim.x) s.rt[i] = f.rt[i];
+}
+
+template <int L>
+__host__ __device__ constexpr size_t fft_table_bytes()
+{
+    // twiddles <= N entries x 6 doubles, flags, perm, REALTR (N/2+1) x 2
+    return (size_t)(L / 2) * 6 * 8 + (size_t)(L / 2) + (size_t)(L / 2) * 4 + (size_t)(L / 4 + 1) * 16 + 64;
+}
+
+template <int L>
+__device__ __forceinline__ FftSmem carve_fft(char *p)
+{
+    constexpr int N = L / 2;
+    FftSmem s;
+    s.tw = (double *)p;
+    p += (size_t)N * 6 * 8;
+    s.rt = (double *)p;
+    p += (size_t)(N / 2 + 1) * 16;
+    s.perm = (int *)p;
+    p += (size_t)N * 4;
+    s.on = (uint8_t *)p;
+    return s;
+}
+
+// One decimation stage S of pot/fft.f FFT on the TC columns of A, then the
+// following stages.
+template <int L, int S, bool FWD>
+__device__ __forceinline__ void stages(double *A, const FftSmem &s, const FftDev &f)
+{
+    using T = Tile<L>;
+    using Sh = Shape<T::N>;
+    if constexpr (S < Sh::nst()) {
+        constexpr int R = Sh::radix(S), H = Sh::span(S), NBF = T::N / R;
+        const int off = f.off[S];
+        for (int w = threadIdx.x; w < NBF * T::TC; w += blockDim.x) {
+            const int c = w % T::TC, bi = w / T::TC;
+            const int j = bi % H, kk = (bi / H) * (R * H) + j;
+            const bool on = s.on[off + j] != 0;
+            const double *tw = s.tw + (size_t)(off + j) * 6;
+            double *a0 = A + (2 * kk) * T::RS + c, *b0 = a0 + T::RS;
+            double *a1 = A + (2 * (kk + H)) * T::RS + c, *b1 = a1 + T::RS;
+            if constexpr (R == 2) {
+                if (!on) {
+                    const double ak = *a1, bk = *b1;
+                    *a1 = *a0 - ak;
+                    *b1 = *b0 - bk;
+                    *a0 = *a0 + ak;
+                    *b0 = *b0 + bk;
+                } else {
+                    const double c1 = tw[0], s1 = tw[1];
+                    const double ak = *a0 - *a1, bk = *b0 - *b1;
+                    *a0 = *a0 + *a1;
+                    *b0 = *b0 + *b1;
+                    *a1 = c1 * ak - s1 * bk;
+                    *b1 = s1 * ak + c1 * bk;
+                }
+            } else {
+                double *a2 = A + (2 * (kk + 2 * H)) * T::RS + c, *b2 = a2 + T::RS;
+                double *a3 = A + (2 * (kk + 3 * H)) * T::RS + c, *b3 = a3 + T::RS;
+                double akp = *a0 + *a2, akm = *a0 - *a2, ajp = *a1 + *a3, ajm = *a1 - *a3;
+                const double A0 = akp + ajp;
+                ajp = akp - ajp;
+                double bkp = *b0 + *b2, bkm = *b0 - *b2, bjp = *b1 + *b3, bjm = *b1 - *b3;
+                const double B0 = bkp + bjp;
+                bjp = bkp - bjp;
+                if constexpr (FWD) {
+                    akp = akm - bjm; akm = akm + bjm; bkp = bkm + ajm; bkm = bkm - ajm;
+                } else {
+                    akp = akm + bjm; akm = akm - bjm; bkp = bkm - ajm; bkm = bkm + ajm;
+                }
+                *a0 = A0;
+                *b0 = B0;
+                if (on) {
+                    *a1 = akp * tw[0] - bkp * tw[1]; *b1 = akp * tw[1] + bkp * tw[0];
+                    *a2 = ajp * tw[2] - bjp * tw[3]; *b2 = ajp * tw[3] + bjp * tw[2];
+                    *a3 = akm * tw[4] - bkm * tw[5]; *b3 = akm * tw[5] + bkm * tw[4];
+                } else {
+                    *a1 = akp; *b1 = bkp; *a2 = ajp; *b2 = bjp; *a3 = akm; *b3 = bkm;
+                }
+            }
+        }
+        __syncthreads();
+        stages<L, S + 1, FWD>(A, s, f);
+    }
+}
+
+// REALTR (pot/fft.f:2-70): the N/2+1 (j, N-j) pairs are independent once the
+// recurrence values are tabulated.
+template <int L>
+__device__ __forceinline__ void realtr_pairs(double *A, const FftSmem &s)
+{
+    using T = Tile<L>;
+    constexpr int n = T::N, nh = n / 2 + 1;
+    for (int w = threadIdx.x; w < nh * T::TC; w += blockDim.x) {
+        const int c = w % T::TC, j = w / T::TC, k = n - j;
+        const double cn = s.rt[2 * j], sn = s.rt[2 * j + 1];
+        const double aj = A[(2 * j) * T::RS + c], bj = A[(2 * j + 1) * T::RS + c];
+        const double ak = A[(2 * k) * T::RS + c], bk = A[(2 * k + 1) * T::RS + c];
+        const double aa = aj + ak, ab = aj - ak, ba = bj + bk, bb = bj - bk;
+        const double re = cn * ba + sn * ab, im = sn * ba - cn * ab;
+        if (j != k) {
+            A[(2 * k + 1) * T::RS + c] = im - bb;
+            A[(2 * k) * T::RS + c] = aa - re;
+        }
+        A[(2 * j + 1) * T::RS + c] = im + bb;
+        A[(2 * j) * T::RS + c] = aa + re;
+    }
+    __syncthreads();
+}
+
+// Forward transform of the TC columns held in A (natural sample order): FFT
+// stages, output permutation (in place through registers), REALTR.  Then row
+// 2q holds A1(q+1) and row 2q+1 holds B1(q+1) of pot/pot3.f:99-100, q = 0..N.
+template <int L>
+__device__ __forceinline__ void forward_columns(double *A, const FftSmem &s, const FftDev &f)
+{
+    using T = Tile<L>;
+    constexpr int NI = (T::N + 1) * T::TC, PER = (NI + 255) / 256;
+    stages<L, 0, true>(A, s, f);
+    double re[PER], im[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+        const int w = threadIdx.x + u * 256;
+        if (w < NI) {
+            const int c = w % T::TC, q = w / T::TC;
+            const int src = s.perm[q < T::N ? q : 0];   // A(N+1) = A(1) (pot/fft.f:44-45)
+            re[u] = A[(2 * src) * T::RS + c];
+            im[u] = A[(2 * src + 1) * T::RS + c];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+        const int w = threadIdx.x + u * 256;
+        if (w < NI) {
+            const int c = w % T::TC, q = w / T::TC;
+            A[(2 * q) * T::RS + c] = re[u];
+            A[(2 * q + 1) * T::RS + c] = im[u];
+        }
+    }
+    __syncthreads();
+    realtr_pairs<L>(A, s);
+}
+
+// Mode l of a transformed column (pot/pot3.f:135-140), before the SF1 scaling.
+template <int L>
+__device__ __forceinline__ double mode_value(const double *A, int l, int c)
+{
+    using T = Tile<L>;
+    return l <= T::N ? A[(2 * l) * T::RS + c] : A[(2 * (l - T::N) + 1) * T::RS + c];
+}
+
+// ---------------------------------------------------------------------------
+// Forward transform of the interior columns + ring moments
+// ---------------------------------------------------------------------------
+// Grid: (ceil(M/TC), NZ, batch).  Reads RHO(2:JMAX, 2:KMAX, :) -- the cells
+// POT3 copies into PHI (pot/pot3.f:70-82) and BDYGEN integrates
+// (pot/boundary.f:366-370) -- and writes X interior plus MOM.
+template <int L>
+__global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work w)
+{
+    using T = Tile<L>;
+    extern __shared__ __align__(16) char smem_raw[];
+    double *A = (double *)smem_raw;
+    double *mtab = A + (size_t)T::ROWS * T::RS;            // [20][L/4] cos, sin of m psi
+    FftSmem fs = carve_fft<L>((char *)(mtab + 20 * (L / 4)));
+    const int J2 = t.J + 2, K2 = t.K + 2;
+    const int j0 = blockIdx.x * T::TC, k = blockIdx.y, b = blockIdx.z;
+    const double *rho = bp.rho[b];
+
+    load_fft_tables(t.fwd, fs);
+    for (int i = threadIdx.x; i < 20 * (L / 4); i += blockDim.x) {
+        const int m = i / (L / 4), l = i % (L / 4);
+        mtab[i] = m < 10 ? t.cosm[(size_t)m * L + l] : t.sinm[(size_t)(m - 10) * L + l];
+    }
+    for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
+        const int c = i % T::TC, l = i / T::TC, j = j0 + c;
+        A[l * T::RS + c] = (j < t.M) ? rho[(size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] : 0.0;
+    }
+    __syncthreads();
+
+    // azimuthal moments of each ring (pot/boundary.f:527-538), before DV, using
+    // psi -> pi - psi, pi + psi, 2 pi - psi to fold the sum to a quarter period
+    {
+        const int c = threadIdx.x / T::TPC, g = threadIdx.x % T::TPC;
+        constexpr int Q = L / 4;
+        double acc[21];
+#pragma unroll
+        for (int q = 0; q < 21; ++q) acc[q] = 0.0;
+        for (int l = g; l < Q; l += T::TPC) {
+            const double r1 = A[l * T::RS + c], r2 = A[(L / 2 - 1 - l) * T::RS + c];
+            const double r3 = A[(L / 2 + l) * T::RS + c], r4 = A[(L - 1 - l) * T::RS + c];
+            const double e = r1 + r4, f = r2 + r3, gg = r1 - r4, h = r3 - r2;
+            const double ce = e + f, co = e - f, se = gg + h, so = gg - h;
+            acc[0] += ce;
+#pragma unroll
+            for (int m = 1; m <= 10; ++m) {
+                acc[m] = __fma_rn(mtab[(m - 1) * Q + l], (m & 1) ? co : ce, acc[m]);
+                acc[10 + m] = __fma_rn(mtab[(9 + m) * Q + l], (m & 1) ? so : se, acc[10 + m]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 21; ++q)
+#pragma unroll
+            for (int o = T::TPC / 2; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        const int j = j0 + c;
+        if (g == 0 && j < t.M) {
+            double *mom = w.mom + (size_t)b * w.smom + (size_t)k * t.M + j;
+#pragma unroll
+            for (int q = 0; q < 21; ++q) mom[(size_t)q * t.nring] = acc[q];
+        }
+    }
+    __syncthreads();
+
+    forward_columns<L>(A, fs, t.fwd);
+
+    double *X = w.X + (size_t)b * w.sX;
+    for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
+        const int c = i % T::TC, l = i / T::TC, j = j0 + c;
+        if (j < t.M) X[((size_t)l * t.K + k) * t.J + j] = mode_value<L>(A, l, c) * t.sf1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Boundary potentials (pot/boundary.f:659-833) and their transform
+// ---------------------------------------------------------------------------
+// Grid: (ceil(njk/8), 1, batch).  For each boundary point: MASSIN/MASSOUT
+// from the prefix/suffix sums and TRMTOT (pot/boundary.f:782-806).  The
+// boundary potential (pot/boundary.f:814-830) is
+//   PHI(psi_l) = -G [c_0 + sum_m (c_m cos m psi_l + s_m sin m psi_l)]
+// with c_0 = sum_L TRMTOT(1,(L,0)), c_m = 2 sum_L TRMTOT(1,(L,m)),
+// s_m = 2 sum_L TRMTOT(2,(L,m)).  POT3 then transforms the boundary columns
+// (pot/pot3.f:93-140); the transform being linear, the modes are the same
+// combination of the recorded transforms of {1, cos m psi, sin m psi}.
+__global__ void __launch_bounds__(256) k_bdy_synth(DevTables t, Work w)
+{
+    constexpr int kPts = 8;
+    __shared__ double trm[kPts][132];
+    __shared__ double cq[kPts][21];
+    __shared__ int colidx[132];
+    const int q0 = blockIdx.x * kPts, b = blockIdx.z, L = t.L;
+    const double *scan = w.scan + (size_t)b * w.sscan;
+
+    for (int i = threadIdx.x; i < 132; i += blockDim.x) colidx[i] = -1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < t.ncol; i += blockDim.x) colidx[t.col_part[i] * 66 + t.col_term[i]] = i;
+    __syncthreads();
+    for (int i = threadIdx.x; i < kPts * 132; i += blockDim.x) {
+        const int c = i / 132, r = i % 132, part = r / 66, term = r % 66, q = q0 + c;
+        double v = 0.0;
+        if (q < t.njk && term < t.ntrm) {
+            const int col = colidx[part * 66 + term];
+            const size_t srow = (size_t)t.jk_sub[q] * 2 * t.ncol;
+            const double min_ = col >= 0 ? scan[srow + col] : 0.0;
+            const double mout = col >= 0 ? scan[srow + t.ncol + col] : 0.0;
+            v = t.jk_bin[(size_t)q * 66 + term] * min_ + t.jk_hout[(size_t)q * 66 + term] * mout;
+        }
+        trm[c][r] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kPts * 21; i += blockDim.x) {
+        const int c = i / 21, q = i % 21;
+        const int m = q <= 10 ? q : q - 10, part = q <= 10 ? 0 : 1;
+        double s = 0.0;
+        for (int ll = m; ll <= t.maxtrm; ++ll) s = s + trm[c][part * 66 + ll * (ll + 1) / 2 + m];
+        cq[c][q] = -t.grav * (q == 0 ? s : 2.0 * s);
+    }
+    __syncthreads();
+    double *X = w.X + (size_t)b * w.sX;
+    for (int i = threadIdx.x; i < kPts * L; i += blockDim.x) {
+        const int c = i / L, l = i % L, q = q0 + c;
+        if (q < t.njk) {
+            double v = 0.0;
+#pragma unroll
+            for (int p = 0; p < 21; ++p) v = __fma_rn(cq[c][p], __ldg(t.fbasis + (size_t)p * L + l), v);
+            X[((size_t)l * t.K + t.jk_k[q]) * t.J + t.jk_j[q]] = v;
+        }
+    }
+}
+
+// /COEFS/ amplitude and phase diagnostics (pot/pot3.f:105-132) of every
+// transformed column of solve 0, read back from X before the mode solve
+// overwrites it.  SF1 = 0.5/N is a power of two, so A1 = X/SF1 exactly.
+// Grid: (ceil(J/32), K), block (32, 8).
+__global__ void k_coef(DevTables t, Work w)
+{
+    const int j = blockIdx.x * 32 + threadIdx.x, k = blockIdx.y, n = t.N;
+    if (j >= t.J) return;
+    const double pi = 3.1415926535897932, inv = 1.0 / t.sf1;
+    const size_t pl = (size_t)t.K * t.J, col = (size_t)k * t.J + j;
+    const int J2 = t.J + 2, K2 = t.K + 2;
+    const size_t ldl = (size_t)J2 * K2, ldi = ldl * (t.L / 2), off = (size_t)(j + 1) + (size_t)J2 * (k + 1);
+    const double a1 = w.X[col] * inv, x1 = fabs(a1);
+    for (int l = 2 + threadIdx.y; l <= n + 1; l += blockDim.y) {
+        if (l <= n) {
+            const double a = w.X[(size_t)(l - 1) * pl + col] * inv, bb = w.X[(size_t)(n + l - 1) * pl + col] * inv;
+            if (x1 != 0.0) w.coef[off + ldl * (l - 2)] = 2.0 * sqrt(a * a + bb * bb) / x1;
+            double philag;
+            if (a > 0.0) philag = atan(bb / a);
+            else if (a < 0.0) philag = atan(bb / a) + pi;
+            else if (bb > 0.0) philag = 0.5 * pi;
+            else if (bb < 0.0) philag = -0.5 * pi;
+            else philag = 4.0 * pi;
+            w.coef[off + ldl * (l - 2) + ldi] = philag * 180. / pi;
+        } else {
+            if (x1 != 0.0) w.coef[off + ldl * (n - 1)] = fabs(w.X[(size_t)n * pl + col] * inv) / x1;
+            w.coef[off + ldl * (n - 1) + ldi] = a1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Inverse transform, ghost cells and z-axis extrapolation
+// ---------------------------------------------------------------------------
+// Grid: (ceil(J/TC), K, batch) over every column POT3 inverts (J = 2..JMAX+1,
+// K = 2..KMAX+1, pot/pot3.f:258-281).  CTAs holding J = 2 also write the axis
+// ghosts (pot/pot3.f:289-292) and the ZAXPHI row PHI(JMAX+2, K, :)
+// (pot/pot3.f:350-387); CTAs at K = 2 write the midplane ghosts
+// (pot/pot3.f:293-296).
+template <int L>
+__global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work w)
+{
+    using T = Tile<L>;
+    constexpr int n = T::N;
+    extern __shared__ __align__(16) char smem_raw[];
+    double *A = (double *)smem_raw;
+    double *red = A + (size_t)T::ROWS * T::RS;   // [L/2] ZAXPHI values
+    FftSmem fs = carve_fft<L>((char *)(red + L / 2));
+    const int J2 = t.J + 2, K2 = t.K + 2;
+    const int j0 = blockIdx.x * T::TC, k = blockIdx.y, b = blockIdx.z;
+    const double *X = w.X + (size_t)b * w.sX;
+    double *phi = bp.phi[b];
+
+    load_fft_tables(t.inv, fs);
+    // A1(1..N+1) = modes 0..N, B1(2..N) = modes N+1..2N-1, B1(1) = B1(N+1) = 0
+    for (int i = threadIdx.x; i < (n + 1) * T::TC; i += blockDim.x) {
+        const int c = i % T::TC, q = i / T::TC, j = j0 + c;
+        double re = 0.0, im = 0.0;
+        if (j < t.J) {
+            const size_t col = (size_t)k * t.J + j, pl = (size_t)t.K * t.J;
+            re = X[(size_t)q * pl + col];
+            if (q >= 1 && q < n) im = X[(size_t)(n + q) * pl + col];
+        }
+        A[(2 * q) * T::RS + c] = re;
+        A[(2 * q + 1) * T::RS + c] = im;
+    }
+    __syncthreads();
+    realtr_pairs<L>(A, fs);
+    stages<L, 0, false>(A, fs, t.inv);
+
+    // sample l of column c in natural order, times SF2 = 0.5 (pot/pot3.f:276-279)
+    auto sample = [&](int l, int c) -> double {
+        const int src = fs.perm[l >> 1];
+        return 0.5 * A[(2 * src + (l & 1)) * T::RS + c];
+    };
+    for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
+        const int c = i % T::TC, l = i / T::TC, j = j0 + c;
+        if (j < t.J) {
+            const double v = sample(l, c);
+            phi[(size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] = v;
+            if (k == 0) phi[(size_t)(j + 1) + (size_t)J2 * ((size_t)K2 * l)] = v;   // PHI(J,1,L)
+        }
+    }
+    if (j0 == 0) {
+        for (int l = threadIdx.x; l < L; l += blockDim.x) {
+            const double v = sample((l + n) % L, 0);                 // PHI(2,K,L+-N)
+            phi[(size_t)J2 * ((k + 1) + (size_t)K2 * l)] = v;       // PHI(1,K,L)
+            if (k == 0) phi[(size_t)J2 * ((size_t)K2 * l)] = v;     // PHI(1,1,L)
+        }
+        // ZAXPHI: Neville extrapolation to r = 0 across +-RHF (pot/pot3.f:354-378)
+        const int lm = L / 2, np = t.npoint;
+        const int ichk = np % 2, num = (np - ichk) / 2, jsp = num + 1;
+        for (int l = threadIdx.x; l < lm; l += blockDim.x) {
+            double p2[11];
+            for (int jj = 2; jj <= jsp; ++jj) {
+                p2[num + (jj - 1)] = sample(l, jj - 2);
+                p2[num - (jj - 2)] = sample(l + lm, jj - 2);
+            }
+            if (ichk == 1) p2[num + num + 1] = sample(l, num);
+            const double xpoint = 0.0;
+            for (int ii = 1; ii <= np - 1; ++ii) {
+                const double p1 = p2[ii], xinv = 1.0 / t.zx[ii], xr = xpoint * xinv;
+                for (int jj = ii + 1; jj <= np; ++jj) {
+                    const double xratio = t.zx[jj] * xinv, pp = p2[jj];
+                    p2[jj] = (p1 * (xratio - xr) + pp * (xr - 1.0)) / (xratio - 1.0);
+                }
+            }
+            const double ph = p2[np];
+            red[l] = ph;
+            phi[(size_t)(t.J + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] = ph;
+            phi[(size_t)(t.J + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * (l + lm))] = ph;
+        }
+        __syncthreads();
+        // PHAC(K): the first largest-|ER| deviation, ER = 1 - PH(L)/PHMAX,
+        // PHMAX the first largest-|PH| value (pot/pot3.f:351,376,381-386)
+        if (threadIdx.x < 32) {
+            double pm = 0.0;
+            int pl = 0x7fffffff;
+            for (int l = threadIdx.x; l < lm; l += 32)
+                if (fabs(red[l]) > fabs(pm)) { pm = red[l]; pl = l; }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double v = __shfl_xor_sync(0xffffffffu, pm, o);
+                const int vl = __shfl_xor_sync(0xffffffffu, pl, o);
+                if (fabs(v) > fabs(pm) || (fabs(v) == fabs(pm) && vl < pl)) { pm = v; pl = vl; }
+            }
+            double em = 0.0;
+            int el = 0x7fffffff;
+            for (int l = threadIdx.x; l < lm; l += 32) {
+                const double er = 1.0 - red[l] / pm;
+                if (fabs(er) > fabs(em)) { em = er; el = l; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double v = __shfl_xor_sync(0xffffffffu, em, o);
+                const int vl = __shfl_xor_sync(0xffffffffu, el, o);
+                if (fabs(v) > fabs(em) || (fabs(v) == fabs(em) && vl < el)) { em = v; el = vl; }
+            }
+            if (threadIdx.x == 0) w.phac[(size_t)b * w.sphac + (k + 2)] = em;
+        }
+    }
+}
+
+// PHICHK / KLOCAT (pot/pot3.f:391-399) and TMASS (pot/boundary.f:554).
+__global__ void k_diag(DevTables t, Work w)
+{
+    const int b = blockIdx.x;
+    if (threadIdx.x != 0) return;
+    const double *phac = w.phac + (size_t)b * w.sphac;
+    double err = 0.0;
+    int klocat = 0;
+    for (int k = 2; k <= t.K + 1; ++k) {
+        const double xx = fabs(phac[k]);
+        if (xx > fabs(err)) { err = phac[k]; klocat = k; }
+    }
+    double *d = w.diag + (size_t)b * w.sdiag;
+    const double *scan = w.scan + (size_t)b * w.sscan;
+    d[0] = scan[(size_t)t.nsub * 2 * t.ncol + 0];   // column 0 = TERM(1)*SUMASS, inside sum over all rings
+    d[1] = err;
+    d[2] = (double)klocat;
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+template <int L>
+static size_t tile_bytes() { return (size_t)Tile<L>::ROWS * Tile<L>::RS * sizeof(double); }
+
+template <int L>
+static cudaError_t forward_l(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s)
+{
+    using T = Tile<L>;
+    const size_t sm = tile_bytes<L>() + (size_t)20 * (L / 4) * 8 + fft_table_bytes<L>();
+    cudaError_t e = ensure_smem((const void *)k_forward<L>, sm);
+    if (e != cudaSuccess) return e;
+    k_forward<L><<<dim3((t.M + T::TC - 1) / T::TC, t.NZ, nb), 256, sm, s>>>(t, bp, w);
+    return cudaGetLastError();
+}
+
+template <int L>
+static cudaError_t inverse_l(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s);
+
+template <int L>
+static cudaError_t inverse_l(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s)
+{
+    using T = Tile<L>;
+    const size_t sm = tile_bytes<L>() + (size_t)(L / 2) * 8 + fft_table_bytes<L>();
+    cudaError_t e = ensure_smem((const void *)k_inverse<L>, sm);
+    if (e != cudaSuccess) return e;
+    k_inverse<L><<<dim3((t.J + T::TC - 1) / T::TC, t.K, nb), 256, sm, s>>>(t, bp, w);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_diag<<<nb, 32, 0, s>>>(t, w);
+    return cudaGetLastError();
+}
+
+#define CHY_DISPATCH_L(FN, ...)                     \
+    switch (t.L) {                                  \
+    case 32: return FN<32>(__VA_ARGS__);            \
+    case 64: return FN<64>(__VA_ARGS__);            \
+    case 128: return FN<128>(__VA_ARGS__);          \
+    case 256: return FN<256>(__VA_ARGS__);          \
+    case 512: return FN<512>(__VA_ARGS__);          \
+    case 1024: return FN<1024>(__VA_ARGS__);        \
+    default: return cudaErrorInvalidValue;          \
+    }
+
+cudaError_t launch_forward(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s)
+{
+    CHY_DISPATCH_L(forward_l, t, bp, w, nb, s)
+}
+
+cudaError_t launch_bdy_synth(const DevTables &t, const Work &w, int nb, cudaStream_t s)
+{
+    k_bdy_synth<<<dim3((t.njk + 7) / 8, 1, nb), 256, 0, s>>>(t, w);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || w.coef == nullptr) return e;
+    k_coef<<<dim3((t.J + 31) / 32, t.K, 1), dim3(32, 8), 0, s>>>(t, w);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_inverse(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s)
+{
+    CHY_DISPATCH_L(inverse_l, t, bp, w, nb, s)
+}
+
+// Compile-time stage structure used by the kernels, for the plan to compare
+// with the recorded schedule.
+template <int L>
+static bool shape_ok(const FftDev &f)
+{
+    using Sh = Shape<L / 2>;
+    if (f.nst != Sh::nst() || f.n != L / 2) return false;
+    for (int s = 0; s < Sh::nst(); ++s)
+        if (f.radix[s] != Sh::radix(s) || f.span[s] != Sh::span(s)) return false;
+    return true;
+}
+
+bool fft_shape_supported(const FftDev &f, int L)
+{
+    switch (L) {
+    case 32: return shape_ok<32>(f);
+    case 64: return shape_ok<64>(f);
+    case 128: return shape_ok<128>(f);
+    case 256: return shape_ok<256>(f);
+    case 512: return shape_ok<512>(f);
+    case 1024: return shape_ok<1024>(f);
+    default: return false;
+    }
+}
+
+}  // namespace chy

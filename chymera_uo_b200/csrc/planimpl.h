@@ -1,0 +1,53 @@
+// planimpl.h -- the plan object behind the C ABI (internal to libchy_pot3).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "chy_pot3.h"
+#include "devplan.h"
+#include "plan.h"
+
+enum ChyStage { ST_FWD = 0, ST_BDY, ST_SYNTH, ST_SOLVE, ST_INV, ST_NSTAGE };
+
+struct MixedState;   // k_mixed.cu
+
+struct chy_plan {
+    chy::HostPlan hp;
+    chy::DevTables t{};
+    int precision = CHY_PREC_FP64;
+    int max_batch = 1;
+    int refine = 1;
+    int num_sms = 148;
+    char *d_tables = nullptr;
+    size_t table_bytes = 0;
+    char *d_work = nullptr;
+    size_t work_bytes = 0;
+    chy::Work w{};
+    size_t nvol = 0;
+    double *stage_rho = nullptr, *stage_phi = nullptr;
+    double *h_diag = nullptr;   // pinned
+    bool profile = false;
+    cudaEvent_t ev[ST_NSTAGE + 1] = {};
+    double stage_ms[ST_NSTAGE] = {};
+    long long stage_calls = 0;
+    long long launches = 0;
+    MixedState *mx = nullptr;
+};
+
+// Mixed-precision mode solve (k_mixed.cu).
+bool chy_mixed_supported(const chy::HostPlan *hp);
+// Appends the mixed path's tables to the packed table image; returns offset.
+size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image);
+void chy_mixed_bind_tables(chy_plan *p, char *dev_base);
+// Extra work-space doubles the mixed path needs (all batch slots).
+size_t chy_mixed_work_doubles(const chy_plan *p);
+void chy_mixed_bind_work(chy_plan *p, double *base);
+// Solves the modes of nb solves in place in X; reports its launch count.
+int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches);
+// After a stream sync: reads the device error word and the per-mode
+// correction norms; CHY_ERR_TIMEOUT if a bounded wait expired.
+int chy_mixed_collect(chy_plan *p, int nb);
+void chy_mixed_fill_diag(const chy_plan *p, int slot, chy_diag *d);
+void chy_mixed_release(chy_plan *p);

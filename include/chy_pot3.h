@@ -1,0 +1,140 @@
+/*
+ * chy_pot3.h -- C ABI of the B200 gravitational-potential solve (CHYMERA pot3).
+ *
+ * One call replaces the reference's SETBDY + BDYGEN + POT3 sequence
+ * (pot/boundary.f:2, pot/boundary.f:88, pot/pot3.f:15) as the ITYPE=71
+ * potential run (radhydro/io.f:212-218) and the per-step update
+ * (radhydro/3dhyd-main.f:474-477) issue it.  Arrays use the reference's
+ * Fortran column-major layout: RHO and PHI are (JMAX+2, KMAX+2, LMAX) doubles
+ * (headers/globals.h:55-58, /POIS/), J fastest.  POT3JMAX = JMAX and
+ * POT3KMAX = KMAX.
+ *
+ * Write-set of a solve (identical to the reference's):
+ *   PHI(1:JMAX+1, 1:KMAX+1, :)  except PHI(JMAX+2, 1, :)   -- written
+ *   PHI(JMAX+2, 2:KMAX+1, :)                                -- written (ZAXPHI)
+ *   PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :)                 -- never touched
+ *   RHO is read-only; only RHO(2:JMAX, 2:KMAX, :) is read.
+ *
+ * No entry point calls exit(); every failure returns a status code.
+ */
+#ifndef CHY_POT3_H
+#define CHY_POT3_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define CHY_OK 0
+/* 1..5 keep the meaning of FISHPACK BLKTRI's IERROR (pot/blktri.f:14-34;
+ * the meanings are spelled out in Poisson/blktri.f90:105-120).  The reference
+ * ignores IERROR (pot/pot3.f:238-239); this library reports it. */
+#define CHY_ERR_M_LT_2 1          /* JMAX-1 < 2 radial unknowns                    */
+#define CHY_ERR_N_NOT_POW2 2      /* KMAX-1 is not 2**k-1 (KMAX not a power of 2)  */
+#define CHY_ERR_EIGEN 4           /* vertical-operator eigen solve failed           */
+#define CHY_ERR_IDIMY 5           /* leading dimension too small                    */
+#define CHY_ERR_ARG 10            /* NULL pointer or invalid argument              */
+#define CHY_ERR_DIMS 11           /* LMAX not a power of 2 (pot/fft.f factor rule), */
+                                  /* or a size out of the supported range          */
+#define CHY_ERR_UNSUPPORTED 12    /* ISYM / MAXTRM / NPOINT outside supported set   */
+#define CHY_ERR_NOT_SETUP 13      /* BDYGEN before SETBDY (pot/boundary.f:311)      */
+#define CHY_ERR_CUDA 20           /* a CUDA runtime call failed                     */
+#define CHY_ERR_NOMEM 21          /* device allocation failed                       */
+#define CHY_ERR_NOCONV 30         /* mixed-precision refinement missed tolerance    */
+#define CHY_ERR_TIMEOUT 31        /* a device-side bounded wait expired             */
+#define CHY_ERR_CAPACITY 32       /* batch larger than the plan's capacity         */
+
+/* ---- descriptors --------------------------------------------------------- */
+enum { CHY_LITERAL_GCC = 0, CHY_LITERAL_R8 = 1 };
+enum { CHY_PREC_FP64 = 0, CHY_PREC_MIXED = 1 };
+enum { CHY_PTR_DEVICE = 0, CHY_PTR_HOST = 1 };
+
+/* Grid and call parameters.  Fields mirror COMMON /GRID/ and /BLOK6/
+ * (headers/globals.h:10,104-109) plus the constant call arguments of
+ * radhydro/3dhyd-main.f:166-167,477 (MAXTRM=10, ISYM=2, NPOINT=8). */
+typedef struct chy_grid {
+    int jmax, kmax, lmax;      /* POT3JMAX=JMAX, POT3KMAX=KMAX, LMAX             */
+    double rof3n, zof3n;       /* radial / vertical spacing (DELR, DELZ)        */
+    const double *r, *z;       /* R(JMAX+2), Z(KMAX+2); NULL: uniform from      */
+    const double *rhf, *zhf;   /* RHF, ZHF;  ROF3N/ZOF3N as radhydro/io.f:194-203 */
+    double pi, grav;           /* PI, GRAV; DTHETA = 2*PI/LMAX (io.f:136-140)   */
+    int isym;                  /* BDYGEN symmetry flag (2 is the production one) */
+    int maxtrm;                /* multipole order l <= MAXTRM (<= 10)           */
+    double redge;              /* BDYGEN REDGE: 0, or R(JMAX+1) per time step   */
+    int npoint;                /* ZAXPHI interpolation points (<= 10)           */
+    int literal_kind;          /* CHY_LITERAL_GCC (chymera-omp) or _R8          */
+} chy_grid;
+
+/* /INSIDE/ diagnostics (pot/boundary.f:112, pot/pot3.f:317) and the
+ * mixed-precision refinement report. */
+typedef struct chy_diag {
+    double tmass;              /* TMASS: total mass seen by BDYGEN              */
+    double phichk;             /* PHICHK: largest z-axis deviation (ZAXPHI)     */
+    int klocat;                /* KLOCAT: K of PHICHK                           */
+    int iterations;            /* approximate solves performed (mixed: 1 +      */
+                               /* corrections; 0 for the FP64 path)             */
+    double corr_rel[8];        /* ||delta_i|| / ||x_{i+1}|| of solve i           */
+} chy_diag;
+
+typedef struct chy_plan chy_plan;
+
+/* Fills a descriptor with the reference's defaults for a JMAX x KMAX x LMAX
+ * grid: ROF3N = 1/JMAX, ZOF3N = 0.5/KMAX, PI = 3.1415926535897932, GRAV = 1,
+ * ISYM = 2, MAXTRM = 10, REDGE = 0, NPOINT = 8, gcc literals. */
+void chy_grid_defaults(chy_grid *g, int jmax, int kmax, int lmax);
+
+/* Builds every per-grid table (FFT schedule, ring and boundary geometry,
+ * stencil, vertical eigenbasis) on the host, uploads them to the current
+ * device and allocates work space for up to max_batch concurrent solves.
+ * Replaces the once-per-run SETBDY(0,ISYM) (pot/boundary.f:2-82) and
+ * BLKTRI(IFLG=0) (pot/blktri.f:13-46). */
+int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **out);
+void chy_plan_destroy(chy_plan *p);
+
+/* One solve: BDYGEN(MAXTRM,ISYM,REDGE) then POT3(NPOINT,IPRINT=0).
+ * rho/phi are device pointers (CHY_PTR_DEVICE) or host pointers
+ * (CHY_PTR_HOST; pinned memory gives full copy bandwidth).  stream may be
+ * NULL (legacy default stream).  diag may be NULL.  For device pointers the
+ * call is asynchronous unless diag is non-NULL. */
+int chy_solve(chy_plan *p, const double *rho, double *phi, chy_diag *diag, int ptr_kind,
+              void *stream);
+
+/* n independent solves of the plan's grid in one launch sequence.  rho[i],
+ * phi[i] as above; diag may be NULL or an array of n. */
+int chy_solve_batch(chy_plan *p, int n, const double *const *rho, double *const *phi,
+                    chy_diag *diag, int ptr_kind, void *stream);
+
+/* Optional /COEFS/ output (pot/pot3.f:105-132): when set, the next solves
+ * also write COEF(JMAX+2, KMAX+2, LMAX/2, 2) (amplitude, phase in degrees)
+ * at coef_dev (device pointer, or NULL to stop). */
+int chy_plan_set_coef(chy_plan *p, double *coef_dev);
+
+/* Fixed number of refinement corrections for CHY_PREC_MIXED (default 1). */
+int chy_plan_set_refine(chy_plan *p, int corrections);
+
+/* Bytes of device work space the plan holds (tables + per-solve scratch). */
+long long chy_plan_device_bytes(const chy_plan *p);
+/* Device work-space bytes one more concurrent solve of this grid needs. */
+long long chy_plan_bytes_per_solve(const chy_plan *p);
+
+const char *chy_status_string(int status);
+/* Message of the last failure on the calling thread, and the CUDA error code
+ * behind the last CHY_ERR_CUDA. */
+const char *chy_last_error(void);
+int chy_last_cuda_error(void);
+
+/* Per-stage device timing with CUDA events recorded on the solve stream:
+ * stage 0 forward transform + ring moments, 1 boundary mass integrals,
+ * 2 boundary potentials + their transform, 3 mode solves, 4 inverse
+ * transform + ghosts + ZAXPHI.  Enabling it synchronises after each batch. */
+int chy_plan_set_profiling(chy_plan *p, int on);
+/* Accumulated milliseconds per stage (n >= 5) and the number of timed
+ * launch sequences; returns the number of stages. */
+int chy_plan_stage_times(const chy_plan *p, double *ms, int n, long long *calls);
+/* Kernel launches this plan has issued so far. */
+long long chy_plan_launch_count(const chy_plan *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,226 @@
+"""libchy_pot3 on the GPU against the CPU oracle, through the C ABI.
+
+Tolerances (relative L2 over every cell of the write set):
+  * plain FP64 path: 1e-12 at 64x32x64.  At 256x128x256 the oracle's own
+    BLKTRI solve of the m = 0 mode is only accurate to ~2.4e-12 (measured
+    against a long-double-refined solution in tests/test_oracle.py), so the
+    bar there is 5e-12; the FP64 path itself is ~10x closer to the exact
+    solution than the oracle.
+  * mixed path (FP16 hi/lo tensor-core transforms, FP32 sweeps, FP64
+    refinement): 1e-10.
+"""
+import functools
+
+import numpy as np
+import pytest
+
+from chymera_uo_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def write_set(J, K):
+    return (slice(0, J + 1), slice(0, K + 1), slice(None))
+
+
+@functools.lru_cache(maxsize=None)
+def oracle_result(cfg, literal="gcc", isym=2, maxtrm=10, redge=0.0, npoint=8, seed_override=None):
+    from oracle import oracle as O
+    if seed_override is None:
+        rho, g = synth.config_density(cfg)
+    else:
+        J, K, L = cfg
+        rho, g = synth.disk_density(J, K, L, seed_override, spiral=True, spectrum=True), synth.default_grid(J, K, L)
+    o = O.Oracle(g.jmax, g.kmax, g.lmax, literal_r8=(literal == "r8"), nthreads=8, want_coef=True)
+    phi = o.solve(rho, isym=isym, maxtrm=maxtrm, redge=redge, npoint=npoint)
+    coef = np.array(o.coef)
+    return rho, phi, o.inside(), coef
+
+
+def gpu_solve(chy, rho, J, K, L, precision="fp64", phi0=None, **gkw):
+    plan = chy.Plan(chy.grid(J, K, L, **gkw), precision, 1)
+    phi = phi0.copy(order="F") if phi0 is not None else np.zeros_like(rho, order="F")
+    (out,), (d,) = plan.solve_batch([rho], [phi], diag=True)
+    return out, d, plan
+
+
+@pytest.mark.parametrize("literal", ["gcc", "r8"])
+def test_fp64_small_grid(chylib, literal):
+    rho, ref, dref, _ = oracle_result(1, literal)
+    phi, d, _ = gpu_solve(chylib, rho, 64, 32, 64, "fp64", literal=literal)
+    ws = write_set(64, 32)
+    assert rel_l2(phi[ws], ref[ws]) < 1e-12
+    assert abs(d["tmass"] - dref["tmass"]) <= 1e-13 * dref["tmass"]
+    assert d["klocat"] == dref["klocat"]
+    assert abs(d["phichk"] - dref["phichk"]) <= 1e-4 * abs(dref["phichk"])
+
+
+def test_fp64_large_grid(chylib):
+    rho, ref, dref, _ = oracle_result(2)
+    phi, d, _ = gpu_solve(chylib, rho, 256, 128, 256, "fp64")
+    ws = write_set(256, 128)
+    assert rel_l2(phi[ws], ref[ws]) < 5e-12
+    assert abs(d["tmass"] - dref["tmass"]) <= 1e-13 * dref["tmass"]
+
+
+@pytest.mark.parametrize("cfg", [1, 2, 3])
+def test_mixed_meets_1e10(chylib, cfg):
+    rho, ref, dref, _ = oracle_result(cfg)
+    g = synth.config_density(cfg)[1]
+    phi, d, _ = gpu_solve(chylib, rho, g.jmax, g.kmax, g.lmax, "mixed")
+    ws = write_set(g.jmax, g.kmax)
+    assert rel_l2(phi[ws], ref[ws]) < 1e-10
+    assert d["iterations"] >= 1 and d["corr_rel"][0] == pytest.approx(1.0)
+
+
+def test_mixed_refinement_converges_geometrically(chylib):
+    rho, ref, _, _ = oracle_result(3)
+    ws = write_set(256, 128)
+    errs = []
+    for corrections in (0, 1, 2):
+        plan = chylib.Plan(chylib.grid(256, 128, 256), "mixed", 1)
+        plan.set_refine(corrections)
+        (phi,), (d,) = plan.solve_batch([rho], diag=True)
+        errs.append(rel_l2(phi[ws], ref[ws]))
+        assert len(d["corr_rel"]) == corrections + 1 or corrections == 0
+    assert errs[0] < 1e-4 and errs[1] < errs[0] * 1e-3 and errs[2] < 1e-11
+
+
+def test_write_set_and_untouched_cells(chylib):
+    """Only the reference's write set changes: PHI(:,KMAX+2,:) and
+    PHI(JMAX+2,1,:) keep the caller's values (radhydro/3dhyd-main.f:457-465
+    zeroes them; POT3/BDYGEN never write them)."""
+    rho, ref, _, _ = oracle_result(1)
+    J, K = 64, 32
+    phi0 = np.full_like(rho, 7.0, order="F")
+    for prec in ("fp64", "mixed"):
+        phi, _, plan = gpu_solve(chylib, rho, J, K, 64, prec, phi0=phi0)
+        assert np.all(phi[:, K + 1, :] == 7.0)
+        assert np.all(phi[J + 1, 0, :] == 7.0)
+        assert np.all(np.isfinite(phi))
+        # the device-pointer path writes the same cells with the same values
+        import torch
+        rd = chylib.to_cuda_fortran(rho)
+        pd = chylib.to_cuda_fortran(phi0)
+        plan.solve(rd, pd)
+        torch.cuda.synchronize()
+        assert np.array_equal(pd.cpu().numpy(), phi)
+
+
+def test_boundary_modes_match_oracle_bdygen(chylib):
+    """X at the boundary = POT3's transform of BDYGEN's boundary values."""
+    from oracle import oracle as O
+    rho, g = synth.config_density(1)
+    J, K, L = 64, 32, 64
+    o = O.Oracle(J, K, L)
+    o.set_grid(1.0 / J, 0.5 / K); o.rho[...] = rho; o.phi[...] = 0.0
+    o.setbdy(0, 2); o.bdygen(10, 2, 0.0)
+    pb = np.array(o.phi)
+    plan = chylib.Plan(chylib.grid(J, K, L), "fp64", 1)
+    plan.solve_batch([rho])
+    X = plan.debug_work("X", L * K * J).reshape(L, K, J)
+    for (j, k) in [(0, K - 1), (J // 2, K - 1), (J - 1, K - 1), (J - 1, 0), (J - 1, K // 2)]:
+        ref = O.forward_real(pb[j + 1, k + 1, :].copy(), False)
+        assert np.abs(X[:, k, j] - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("isym,maxtrm,npoint,redge", [(1, 10, 8, 0.0), (3, 8, 8, 0.0), (2, 4, 7, 0.0),
+                                                      (-2, 10, 8, 0.0), (2, 10, 8, 0.6)])
+def test_call_parameter_variants(chylib, isym, maxtrm, npoint, redge):
+    """ISYM, MAXTRM, NPOINT and REDGE as BDYGEN/ZAXPHI accept them
+    (pot/boundary.f:97-105, pot/pot3.f:328-348)."""
+    rho, ref, dref, _ = oracle_result(1, "gcc", isym, maxtrm, redge, npoint)
+    phi, d, _ = gpu_solve(chylib, rho, 64, 32, 64, "fp64", isym=isym, maxtrm=maxtrm, npoint=npoint, redge=redge)
+    ws = write_set(64, 32)
+    assert rel_l2(phi[ws], ref[ws]) < 1e-12
+    assert abs(d["tmass"] - dref["tmass"]) <= 1e-12 * abs(dref["tmass"])
+
+
+@pytest.mark.parametrize("J,K,L", [(128, 64, 128), (64, 32, 256), (256, 64, 64)])
+def test_other_grid_sizes(chylib, J, K, L):
+    rho, ref, _, _ = oracle_result((J, K, L), seed_override=21)
+    for prec, tol in (("fp64", 2e-12), ("mixed", 1e-10)):
+        phi, _, _ = gpu_solve(chylib, rho, J, K, L, prec)
+        ws = write_set(J, K)
+        assert rel_l2(phi[ws], ref[ws]) < tol, prec
+
+
+def test_batch_results_equal_single_solves_bitwise(chylib):
+    """Each result is the same alone and in a batch: every reduction has a
+    fixed order, nothing depends on scheduling."""
+    import torch
+    J, K, L = 64, 32, 64
+    rhos = [synth.disk_density(J, K, L, s, spiral=True, spectrum=True) for s in range(5)]
+    for prec in ("fp64", "mixed"):
+        plan = chylib.Plan(chylib.grid(J, K, L), prec, 8)
+        rd = [chylib.to_cuda_fortran(r) for r in rhos]
+        batch = plan.solve_batch(rd)
+        torch.cuda.synchronize()
+        for r, b in zip(rd, batch):
+            single = plan.solve(r)
+            torch.cuda.synchronize()
+            assert torch.equal(single, b)
+
+
+def test_coef_diagnostics(chylib):
+    """/COEFS/ amplitude and phase (pot/pot3.f:105-132)."""
+    import torch
+    rho, _, _, coef_ref = oracle_result(1)
+    J, K, L = 64, 32, 64
+    plan = chylib.Plan(chylib.grid(J, K, L), "fp64", 1)
+    coef = torch.zeros((2, L // 2, K + 2, J + 2), dtype=torch.float64, device="cuda").permute(3, 2, 1, 0)
+    plan.set_coef(coef)
+    plan.solve(chylib.to_cuda_fortran(rho))
+    torch.cuda.synchronize()
+    got = coef.cpu().numpy()
+    sel = (slice(1, J + 1), slice(1, K + 1))
+    amp, ph = got[sel + (slice(None), 0)], got[sel + (slice(None), 1)]
+    amp_r, ph_r = coef_ref[sel + (slice(None), 0)], coef_ref[sel + (slice(None), 1)]
+    assert np.abs(amp - amp_r).max() <= 1e-9 * np.abs(amp_r).max()
+    # COEF(J,K,N,2) holds A1(1), the raw m = 0 coefficient
+    assert np.abs(ph[..., -1] - ph_r[..., -1]).max() <= 1e-12 * np.abs(ph_r[..., -1]).max()
+    # a phase is only as well defined as its amplitude: an error e in the
+    # transform moves it by ~e/amplitude radians, so compare where the
+    # amplitude (relative to m = 0) is above 1e-6, modulo 360 degrees
+    mask = amp_r[..., :-1] > 1e-6
+    d = np.abs(ph[..., :-1] - ph_r[..., :-1])[mask]
+    d = np.minimum(d, np.abs(d - 360.0))
+    assert mask.sum() > 1000 and d.max() <= 1e-4
+
+
+def test_tensor_core_tile_product(chylib):
+    """One tcgen05 tile product (FP16 hi/lo, three passes) against FP64."""
+    import ctypes as C
+    import torch
+    J, K, L = 256, 128, 256
+    g = chylib.grid(J, K, L)
+    plan = chylib.Plan(g, "mixed", 1)
+    NZ = K - 1
+    out = np.zeros(NZ * NZ)
+    chylib.lib().chy_dbg_table(C.byref(g), b"U", out.ctypes.data_as(C.POINTER(C.c_double)), NZ * NZ)
+    U = out.reshape(NZ, NZ)
+    for NT in (64, 256):
+        Bm = np.zeros((NT, 128), np.float32)
+        Bm[:, :NZ] = np.random.default_rng(NT).uniform(-2000, 2000, (NT, NZ))
+        Bd = torch.from_numpy(Bm).cuda()
+        Dd = torch.zeros((128, NT), dtype=torch.float32, device="cuda")
+        assert chylib.lib().chy_dbg_umma(plan._p, 0, Bd.data_ptr(), Dd.data_ptr(), NT) == 0
+        ref = np.zeros((128, 128)); ref[:NZ, :NZ] = U
+        ref = 4096.0 * ref @ Bm.astype(np.float64).T
+        assert np.abs(Dd.cpu().numpy() - ref).max() <= 5e-6 * np.abs(ref).max()
+
+
+def test_status_codes_on_device(chylib):
+    import ctypes as C
+    L = chylib.lib()
+    p = C.c_void_p()
+    g = chylib.grid(64, 48, 64)     # KMAX not a power of two
+    assert L.chy_plan_create(C.byref(g), 0, 1, C.byref(p)) == 2
+    g = chylib.grid(64, 32, 64)
+    assert L.chy_plan_create(C.byref(g), 0, 1, C.byref(p)) == 0
+    assert L.chy_solve(p, None, None, None, 0, None) == 10
+    L.chy_plan_destroy(p)

@@ -1,0 +1,128 @@
+"""Host-side parts of libchy_pot3, checked without a GPU: the recorded
+transform schedule against the oracle, the plan tables, and the C ABI's
+exported symbols and argument checking."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def table(chy, g, name, n):
+    out = np.zeros(n)
+    m = chy.lib().chy_dbg_table(C.byref(g), name.encode(), dp(out), n)
+    assert m >= 0, (name, m)
+    return out[:m]
+
+
+@pytest.mark.parametrize("n", [16, 32, 64, 128, 256, 512])
+@pytest.mark.parametrize("isn", [1, -1])
+@pytest.mark.parametrize("lit", [0, 1])
+def test_recorded_schedule_is_bitwise_the_oracle_fft(chylib, ora, n, isn, lit):
+    """The stage/twiddle/permutation tables the device transforms execute,
+    applied on the host, reproduce pot/fft.f FFT and REALTR bit for bit."""
+    rng = np.random.default_rng(n * 7 + isn + lit)
+    a, b = rng.standard_normal(n + 1), rng.standard_normal(n + 1)
+    a1, b1, a2, b2 = a.copy(), b.copy(), a.copy(), b.copy()
+    assert chylib.lib().chy_dbg_fft(n, isn, lit, dp(a1), dp(b1)) == 0
+    ora.fft(a2, b2, isn, bool(lit), n)
+    assert np.array_equal(a1[:n], a2[:n]) and np.array_equal(b1[:n], b2[:n])
+    a3, b3, a4, b4 = a.copy(), b.copy(), a.copy(), b.copy()
+    assert chylib.lib().chy_dbg_realtr(n, isn, lit, dp(a3), dp(b3)) == 0
+    ora.realtr(a4, b4, n, isn, bool(lit))
+    assert np.array_equal(a3, a4) and np.array_equal(b3, b4)
+
+
+def test_schedule_rejects_non_power_of_two(chylib):
+    a = np.zeros(13); b = np.zeros(13)
+    assert chylib.lib().chy_dbg_fft(12, 1, 0, dp(a), dp(b)) == 11   # CHY_ERR_DIMS
+
+
+@pytest.mark.parametrize("J,K,L", [(64, 32, 64), (256, 128, 256), (128, 64, 128)])
+def test_vertical_eigenbasis(chylib, J, K, L):
+    g = chylib.grid(J, K, L)
+    NZ = K - 1
+    U = table(chylib, g, "U", NZ * NZ).reshape(NZ, NZ)
+    V = table(chylib, g, "V", NZ * NZ).reshape(NZ, NZ)
+    lam = table(chylib, g, "lam", NZ)
+    an, bn, cn = table(chylib, g, "an", NZ), table(chylib, g, "bn", NZ), table(chylib, g, "cn", NZ)
+    Tz = np.diag(bn) + np.diag(an[1:], -1) + np.diag(cn[:-1], 1)
+    assert np.abs(U @ V - np.eye(NZ)).max() < 1e-13
+    assert np.abs(V @ np.diag(lam) @ U - Tz).max() < 1e-13 * np.abs(Tz).max()
+    assert np.all(lam < 0)   # Neumann midplane + Dirichlet top: negative definite
+
+
+def test_stencil_matches_pot3_formulas(chylib):
+    from tests.test_oracle import pot3_operator
+    J, K, L = 64, 32, 64
+    g = chylib.grid(J, K, L)
+    op = pot3_operator(J, K, L, 0)
+    for name in ("an", "bn", "cn", "am", "cm"):
+        got = table(chylib, g, name, 256)
+        assert np.array_equal(got, op[name]), name
+    sc = table(chylib, g, "scalars", 8)
+    assert sc[2] == op["cmmax"] and sc[3] == op["ammin"] and sc[4] == op["cnmax"]
+
+
+def test_boundary_splits_are_sorted_ring_counts(chylib):
+    """jk_split = number of rings with RSPHER <= RBDY(JK) (pot/boundary.f:561),
+    counted on the reference's own FP64 expressions."""
+    J, K, L = 64, 32, 64
+    g = chylib.grid(J, K, L)
+    rs = table(chylib, g, "ring_rsph", (J - 1) * (K - 1))
+    split = table(chylib, g, "jk_split", J + K)
+    from chymera_uo_b200 import synth
+    gg = synth.default_grid(J, K, L)
+    rhf, zhf = gg.rhf(), gg.zhf()
+    zk2 = zhf[K] * zhf[K]
+    rb = [np.sqrt(zk2 + rhf[j - 1] * rhf[j - 1]) for j in range(2, J + 2)]
+    rj2 = rhf[J] * rhf[J]
+    rb += [np.sqrt(rj2 + zhf[k - 1] * zhf[k - 1]) for k in range(2, K + 1)]
+    assert len(split) == len(rb)
+    for q, r in enumerate(rb):
+        assert split[q] == np.count_nonzero(rs <= r)
+
+
+def test_rejects_unsupported_grids(chylib):
+    out = np.zeros(4)
+    for (J, K, L), code in [((64, 48, 64), 2), ((64, 32, 48), 11), ((2, 32, 64), 1)]:
+        g = chylib.grid(J, K, L)
+        assert chylib.lib().chy_dbg_table(C.byref(g), b"lam", dp(out), 4) == -code
+    g = chylib.grid(64, 32, 64, isym=5)
+    assert chylib.lib().chy_dbg_table(C.byref(g), b"lam", dp(out), 4) == -12
+
+
+def _header_functions():
+    names = []
+    for h in ("chy_pot3.h", "chy_pot3_testing.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"\b(chy_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(chylib):
+    names = _header_functions()
+    assert "chy_solve" in names and "chy_plan_create" in names
+    lib = C.CDLL(chylib.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_argument_checks(chylib):
+    L = chylib.lib()
+    assert L.chy_status_string(0) == b"ok"
+    assert b"BLKTRI IERROR=2" in L.chy_status_string(2)
+    p = C.c_void_p()
+    assert L.chy_plan_create(None, 0, 1, C.byref(p)) == 10
+    g = chylib.grid(64, 32, 64)
+    assert L.chy_plan_create(C.byref(g), 7, 1, C.byref(p)) == 10
+    assert L.chy_plan_create(C.byref(g), 0, 0, C.byref(p)) == 10
+    assert L.chy_solve(None, None, None, None, 0, None) == 10

@@ -1,0 +1,291 @@
+"""The CPU oracle checked against independent references.
+
+The reference ships no tests, fixtures or outputs and cannot be built here
+(Fortran, no compiler), so the restatement is pinned by mathematics:
+  * FFT/REALTR against numpy's real FFT (exact in -r8 literal mode, and the
+    gcc-literal mode's single-precision-angle error quantified);
+  * BLKTRI against scipy sparse LU on the same block-tridiagonal systems,
+    including the real POT3 operators with a long-double-refined solution;
+  * POT3 against a manufactured solution of its own discrete operator;
+  * BDYGEN against multipole known answers;
+  * the committed regression fixtures (tests/golden/).
+"""
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spl
+
+from chymera_uo_b200 import synth
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+# ---------------------------------------------------------------------------
+# FFT / REALTR (pot/fft.f)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("n", [2, 4, 8, 16, 32, 64, 128, 256, 512])
+def test_fft_matches_numpy_exp_plus(ora, n):
+    """FFT(A,B,N,N,N,+1) is the exp(+i) DFT (pot/fft.f:91-92)."""
+    rng = np.random.default_rng(n)
+    a, b = rng.standard_normal(n), rng.standard_normal(n)
+    A, B = a.copy(), b.copy()
+    ora.fft(A, B, 1, True)
+    ref = np.fft.ifft(a + 1j * b) * n
+    assert np.abs(A + 1j * B - ref).max() <= 1e-13 * np.abs(ref).max()
+    A, B = a.copy(), b.copy()
+    ora.fft(A, B, -1, True)
+    ref = np.fft.fft(a + 1j * b)
+    assert np.abs(A + 1j * B - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("L", [32, 64, 128, 256, 512])
+def test_realtr_r8_equals_rfft(ora, L):
+    """POT3's forward transform with -r8 literals: cosine coefficients
+    Re(rfft)/N and sine coefficients -Im(rfft)/N (pot/pot3.f:95-140)."""
+    x = np.random.default_rng(L).standard_normal(L)
+    m = ora.forward_real(x, True)
+    n = L // 2
+    ref = np.fft.rfft(x)
+    assert np.abs(m[: n + 1] - ref.real / n).max() < 1e-14 * np.abs(x).max() * 4
+    assert np.abs(m[n + 1:] + ref.imag[1:n] / n).max() < 1e-14 * np.abs(x).max() * 4
+
+
+@pytest.mark.parametrize("L", [64, 128, 256])
+def test_gcc_literal_transform_differs_by_single_precision_pi(ora, L):
+    """gcc-literal builds take the twiddle angle from REAL(4) ATAN(1.0)
+    (pot/fft.f:38,129): the transform differs from the exact DFT at ~1e-7.
+    The -r8 pair round-trips to rounding; the gcc pair does only when every
+    stage is radix 4 (LMAX = 128): radix-2 stages rotate the partner of
+    position j by the true pi (pot/fft.f:221-224), so the gcc forward and
+    inverse transforms are not exact inverses -- which is why refinement has to
+    work on the mode-space equations."""
+    x = np.random.default_rng(7).standard_normal(L)
+    g = ora.forward_real(x, False)
+    r = ora.forward_real(x, True)
+    rel = np.abs(g - r).max() / np.abs(r).max()
+    assert 1e-9 < rel < 1e-6
+    assert np.abs(ora.inverse_real(r, True) - x).max() < 1e-14 * 8
+    rt = np.abs(ora.inverse_real(g, False) - x).max()
+    if L == 128:
+        assert rt < 1e-14 * 8
+    else:
+        assert 1e-10 < rt < 1e-6
+
+
+# ---------------------------------------------------------------------------
+# BLKTRI (pot/blktri.f)
+# ---------------------------------------------------------------------------
+def _assemble(an, bn, cn, am, bm, cm):
+    M, N = len(am), len(an)
+    Tm = sp.diags([am[1:], bm, cm[:-1]], [-1, 0, 1])
+    Tn = sp.diags([an[1:], bn, cn[:-1]], [-1, 0, 1])
+    return (sp.kron(Tn, sp.eye(M)) + sp.kron(sp.eye(N), Tm)).tocsc()
+
+
+@pytest.mark.parametrize("M,N", [(15, 7), (63, 31), (255, 127)])
+def test_blktri_random_systems(ora, M, N):
+    rng = np.random.default_rng(M)
+    an, cn = rng.uniform(0.5, 1.5, N), rng.uniform(0.5, 1.5, N)
+    bn = -(an + cn) - rng.uniform(0, 1, N)
+    an[0] = cn[-1] = 0
+    am, cm = rng.uniform(0.5, 1.5, M), rng.uniform(0.5, 1.5, M)
+    bm = -(am + cm) - rng.uniform(0, 1, M)
+    am[0] = cm[-1] = 0
+    y = rng.standard_normal((M, N))
+    x, ierr = ora.blktri_solve(an, bn, cn, am, bm, cm, y.copy(order="F"))
+    assert ierr == 0
+    xs = spl.spsolve(_assemble(an, bn, cn, am, bm, cm), y.flatten(order="F")).reshape((M, N), order="F")
+    assert np.linalg.norm(x - xs) / np.linalg.norm(xs) < 1e-13
+
+
+def test_blktri_error_codes(ora):
+    """IERROR 2: N not 2**k-1 (pot/blktri.f:29-31)."""
+    M, N = 15, 6
+    an = np.ones(N); cn = np.ones(N); bn = -3 * np.ones(N)
+    am = np.ones(M); cm = np.ones(M); bm = -3 * np.ones(M)
+    _, ierr = ora.blktri_solve(an, bn, cn, am, bm, cm, np.zeros((M, N), order="F"))
+    assert ierr == 2
+
+
+def pot3_operator(J, K, L, m, lit=False):
+    """POT3's mode-m operator coefficients (pot/pot3.f:158-230), numpy."""
+    g = synth.default_grid(J, K, L)
+    rhf, zhf = g.rhf(), g.zhf()
+    RHF = lambda j: rhf[j - 1]
+    ZHF = lambda k: zhf[k - 1]
+    dth = g.dtheta
+    rd2 = np.zeros(J + 1); rd3 = np.zeros(J + 1); den = np.zeros(J + 1)
+    rd2[1] = 0.5 / RHF(2); rd3[1] = 1.0 / RHF(1)
+    for j in range(2, J + 1):
+        den[j] = 1.0 / (RHF(j + 1) - RHF(j - 1)); rd2[j] = 1.0 / (RHF(j + 1) - RHF(j)); rd3[j] = 1.0 / RHF(j)
+    zd2 = np.zeros(K + 1); dz = np.zeros(K + 1)
+    zd2[1] = 0.5 / ZHF(2)
+    for k in range(2, K + 1):
+        dz[k] = 1.0 / (ZHF(k + 1) - ZHF(k - 1)); zd2[k] = 1.0 / (ZHF(k + 1) - ZHF(k))
+    cm = np.array([2. * (rd2[j] + 0.5 * rd3[j]) * den[j] for j in range(2, J + 1)])
+    am = np.array([2. * (rd2[j - 1] - 0.5 * rd3[j]) * den[j] for j in range(2, J + 1)])
+    c = np.array([rd3[j] * rd3[j] / (dth * dth) for j in range(2, J + 1)])
+    cn = np.array([2. * zd2[k] * dz[k] for k in range(2, K + 1)])
+    an = np.array([2. * zd2[k - 1] * dz[k] for k in range(2, K + 1)])
+    bn = -cn - an
+    cmmax, ammin, cnmax = cm[-1], am[0], cn[-1]
+    cm[-1] = 0; am[0] = 0; cn[-1] = 0; bn[0] = -cn[0]; an[0] = 0
+    xl = np.cos(m * dth)
+    bm = -cm - am + 2 * (xl - 1) * c
+    bm[0] = -cm[0] + ((-1.0) ** m - 1) * ammin + 2 * (xl - 1) * c[0]
+    bm[-1] = -cmmax - am[-1] + 2 * (xl - 1) * c[-1]
+    return dict(an=an, bn=bn, cn=cn, am=am, bm=bm, cm=cm, c=c, cmmax=cmmax, ammin=ammin, cnmax=cnmax)
+
+
+@pytest.mark.parametrize("m", [0, 1, 16, 128])
+def test_blktri_pot3_operator_accuracy(ora, m):
+    """On the 256x128 POT3 operators BLKTRI agrees with a long-double
+    refined sparse solution.  Its own error is largest for the m=0 mode
+    (about 2.4e-12 relative L2): the floor any FP64 reimplementation is
+    compared against."""
+    J, K = 256, 128
+    op = pot3_operator(J, K, 256, m)
+    M, N = J - 1, K - 1
+    jj = np.arange(M)[:, None]; kk = np.arange(N)[None, :]
+    y = np.exp(-((jj - 40) / 30.0) ** 2 - (kk / 20.0) ** 2) * (1 + 0.1 * np.random.default_rng(0).standard_normal((M, N)))
+    A = _assemble(op["an"], op["bn"], op["cn"], op["am"], op["bm"], op["cm"])
+    lu = spl.splu(A)
+    b = y.flatten(order="F")
+    x = lu.solve(b)
+    Al = A.astype(np.longdouble)
+    for _ in range(3):
+        r = b.astype(np.longdouble) - Al @ x.astype(np.longdouble)
+        x = x + lu.solve(r.astype(np.float64))
+    xt = x.reshape((M, N), order="F")
+    xb, ierr = ora.blktri_solve(op["an"], op["bn"], op["cn"], op["am"], op["bm"], op["cm"], y.copy(order="F"))
+    assert ierr == 0
+    err = np.linalg.norm(xb - xt) / np.linalg.norm(xt)
+    assert err < 5e-12
+
+
+# ---------------------------------------------------------------------------
+# POT3 against a manufactured solution of its discrete operator
+# ---------------------------------------------------------------------------
+def apply_pot3_operator(phi, J, K, L):
+    """The real-space 7-point operator POT3 inverts (pot/pot3.f:158-230),
+    applied to a full PHI array: radial AM/CM, vertical AN/CN, azimuthal
+    C(J)(PHI(L+1) - 2 PHI(L) + PHI(L-1)), the axis ghost PHI(1,K,L) =
+    PHI(2,K,L+N), the midplane ghost PHI(J,1,L) = PHI(J,2,L), Dirichlet
+    values at J = JMAX+1 and K = KMAX+1.  Returns A(phi) on the interior."""
+    op = pot3_operator(J, K, L, 0)
+    N = L // 2
+    M, NZ = J - 1, K - 1
+    P = phi[1:J, 1:K, :]                       # interior (j=2..J, k=2..K)
+    out = np.zeros_like(P)
+    am = np.r_[op["ammin"], op["am"][1:]][:, None, None]
+    cmr = np.r_[op["cm"][:-1], op["cmmax"]][:, None, None]
+    up = np.concatenate([phi[2:J + 1, 1:K, :]], axis=0)         # j+1 (J+1 is the boundary)
+    axis = np.roll(phi[1:2, 1:K, :], -N, axis=2)                # PHI(2,K,L+N)
+    down = np.concatenate([axis, phi[1:J - 1, 1:K, :]], axis=0)  # j-1
+    out += am * down + cmr * up - (am + cmr) * P
+    c = op["c"][:, None, None]
+    out += c * (np.roll(P, -1, axis=2) - 2 * P + np.roll(P, 1, axis=2))
+    an = np.r_[0.0, op["an"][1:]][None, :, None]
+    cnr = np.r_[op["cn"][:-1], op["cnmax"]][None, :, None]
+    zup = phi[1:J, 2:K + 1, :]
+    zdn = np.concatenate([phi[1:J, 1:2, :], phi[1:J, 1:K - 1, :]], axis=1)   # midplane ghost = PHI(J,2)
+    cn0 = op["cn"][0]
+    anr = np.r_[cn0, op["an"][1:]][None, :, None]   # at k=1 the ghost term uses CN(1)
+    out += anr * zdn + cnr * zup - (anr + cnr) * P
+    return out
+
+
+def test_pot3_manufactured_solution(ora):
+    """With -r8 literals POT3 inverts its 7-point operator exactly: choose
+    PHI, set RHO = A(PHI)/(4 pi G) and the Dirichlet boundary values, run
+    POT3 alone, and recover PHI."""
+    J, K, L = 32, 16, 32
+    g = synth.default_grid(J, K, L)
+    r = g.rhf()[:, None, None]; z = g.zhf()[None, :, None]
+    psi = ((np.arange(L) + 0.5) * g.dtheta)[None, None, :]
+    phi = (np.exp(-(r ** 2 + z ** 2)) * (1 + 0.3 * np.cos(2 * psi) * r ** 2 + 0.1 * np.sin(3 * psi) * r ** 3)
+           ).astype(np.float64)
+    phi = np.asfortranarray(phi)
+    A = apply_pot3_operator(phi, J, K, L)
+    o = ora.Oracle(J, K, L, literal_r8=True)
+    o.set_grid(1.0 / J, 0.5 / K)
+    rho = np.zeros((J + 2, K + 2, L), order="F")
+    rho[1:J, 1:K, :] = A / (4.0 * np.pi)
+    o.rho[...] = rho
+    o.phi[...] = 0.0
+    o.phi[J, 1:K + 1, :] = phi[J, 1:K + 1, :]     # outer boundary J = JMAX+1
+    o.phi[1:J + 1, K, :] = phi[1:J + 1, K, :]     # top boundary K = KMAX+1
+    o.pot3(8, 0)
+    got = np.array(o.phi)
+    err = np.abs(got[1:J, 1:K, :] - phi[1:J, 1:K, :]).max() / np.abs(phi).max()
+    assert err < 1e-12
+
+
+# ---------------------------------------------------------------------------
+# BDYGEN multipole known answers (pot/boundary.f)
+# ---------------------------------------------------------------------------
+def _boundary_values(ora, rho, J, K, L, **kw):
+    o = ora.Oracle(J, K, L)
+    o.set_grid(1.0 / J, 0.5 / K)
+    o.rho[...] = rho
+    o.phi[...] = 0.0
+    o.setbdy(0, kw.get("isym", 2))
+    assert o.bdygen(kw.get("maxtrm", 10), kw.get("isym", 2), 0.0) == 0
+    return np.array(o.phi), o.inside(), np.array(o.rbdy)
+
+
+def test_bdygen_compact_mass_is_monopole(ora):
+    """A compact mass near the origin gives PHI ~ -G M / r on the boundary."""
+    J, K, L = 64, 32, 64
+    rho = np.zeros((J + 2, K + 2, L), order="F")
+    rho[1:3, 1:3, :] = 1.0
+    phi, d, rb = _boundary_values(ora, rho, J, K, L)
+    top = phi[1:J + 1, K, 0]
+    rtop = rb[:J]
+    assert np.allclose(top, -d["tmass"] / rtop, rtol=2e-3)
+
+
+def test_bdygen_axisymmetric_density_gives_axisymmetric_boundary(ora):
+    J, K, L = 64, 32, 64
+    rho = synth.disk_density(J, K, L, 5, noise=0.0)
+    phi, _, _ = _boundary_values(ora, rho, J, K, L)
+    top = phi[1:J + 1, K, :]
+    assert np.abs(top - top[:, :1]).max() <= 1e-13 * np.abs(top).max()
+
+
+def test_bdygen_pure_azimuthal_mode(ora):
+    """rho = rho0(r,z) (1 + eps cos 3 psi) puts boundary power only in m = 0, 3."""
+    J, K, L = 64, 32, 64
+    base = synth.disk_density(J, K, L, 5, noise=0.0)
+    psi = (np.arange(1, L + 1) - 0.5) * 2 * np.pi / L
+    rho = np.asfortranarray(base * (1 + 0.2 * np.cos(3 * psi))[None, None, :])
+    phi, _, _ = _boundary_values(ora, rho, J, K, L)
+    spec = np.abs(np.fft.rfft(phi[1:J + 1, K, :], axis=1)).max(axis=0)
+    others = np.delete(spec, [0, 3])
+    assert others.max() < 1e-10 * spec[3]
+
+
+# ---------------------------------------------------------------------------
+# Regression fixtures
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["disk_32x16x32_gcc", "disk_32x16x32_r8", "disk_32x16x32_isym1_m8_np7"])
+def test_oracle_matches_fixture(ora, name):
+    f = np.load(os.path.join(GOLDEN, name + ".npz"))
+    J, K, L = int(f["J"]), int(f["K"]), int(f["L"])
+    rho = synth.disk_density(J, K, L, int(f["seed"]), spiral=True, spectrum=True)
+    o = ora.Oracle(J, K, L, literal_r8=bool(f["r8"]))
+    phi = o.solve(rho, isym=int(f["isym"]), maxtrm=int(f["maxtrm"]), redge=float(f["redge"]),
+                  npoint=int(f["npoint"]))
+    assert np.array_equal(phi, f["phi"])
+    d = o.inside()
+    assert d["tmass"] == float(f["tmass"]) and d["klocat"] == int(f["klocat"])
+
+
+def test_oracle_threads_agree_with_serial(ora):
+    """The OpenMP merge order changes BDYGEN's sums only at rounding level."""
+    rho, g = synth.config_density(1)
+    p1 = ora.Oracle(64, 32, 64, nthreads=1).solve(rho)
+    p4 = ora.Oracle(64, 32, 64, nthreads=4).solve(rho)
+    assert np.linalg.norm(p4 - p1) / np.linalg.norm(p1) < 1e-13
