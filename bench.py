@@ -1,0 +1,397 @@
+"""pot3 throughput bench: solves/s of the mixed-precision B200 pot3 at
+JMAX x KMAX x LMAX = 256 x 128 x 256 (SETBDY + BDYGEN + POT3 of the
+reference, pot/boundary.f and pot/pot3.f), with p50/p99 single-solve latency,
+the plain FP64 GPU path on the same inputs, and accuracy against both.
+
+One step = one batched launch sequence over --batch independent seeded disk
+densities (m=2 spiral + m<=32 spectrum), inputs and outputs resident in HBM
+(B x 137 MB, far larger than the 126 MB L2, so nothing is re-read from L2
+across steps).  `e2e` is the same metric through the public API with pinned
+host buffers, host<->device copies inside the timed region.
+
+    python bench.py [--gpus N --steps K --warmup W --batch B]
+    python bench.py --impl reference      # the CPU restatement on host cores
+
+Multi-GPU (torchrun): every rank solves its own densities; there is no
+exchange step in a pot3 solve, so ranks are replicas (weak scaling), timed
+between barriers with the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+J, K, L = 256, 128, 256
+METRIC = "pot3 solves/s @256x128x256 mixed vs FP64 (rel L2≤1e-10); p50/p99 latency"
+UNIT = "solves/s"
+WORKLOAD = "pot3 256x128x256 mixed precision, seeded disks: m=2 spiral + m<=32 spectrum"
+SEED0 = 3
+SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+
+def densities(n, first):
+    from chymera_uo_b200 import synth
+    return [synth.disk_density(J, K, L, SEED0 + 7919 * (first + i), spiral=True, spectrum=True)
+            for i in range(n)]
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- helpers
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), ws
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={SMI_FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.index)], stdout=self.out, stderr=subprocess.DEVNULL)
+            t0 = time.time()
+            while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.05)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), float(f[3]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        busy = [r for r in rows if r[2] > 200.0] or rows
+        reasons = sorted({REASONS[i] for r in busy for i, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in busy])), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(busy),
+                "power_w_median": float(np.median([r[2] for r in busy]))}
+
+
+def peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic_per_solve():
+    """DRAM bytes (read + write) per solve of the mode-solve kernel from the
+    committed ncu summary of that kernel, or None."""
+    path = os.path.join(HERE, "profiles", "k_mode_mixed_256x128x256.md")
+    try:
+        m = re.search(r"dram_bytes_per_solve:\s*([0-9]+)", open(path).read())
+    except OSError:
+        return None
+    return int(m.group(1)) if m else None
+
+
+def mode_solve_bytes_per_solve():
+    """Algorithmic HBM bytes of the mode-solve kernel per solve: it reads the
+    transformed right-hand side X (LMAX x KMAX x JMAX doubles, the boundary
+    row and column included) once and writes the interior modes
+    (LMAX x (KMAX-1) x (JMAX-1) doubles) once."""
+    return 8 * L * K * J + 8 * L * (K - 1) * (J - 1)
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank, _, ws = dist_info()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    cores = host_threads()
+    rho = densities(1, 0)[0]
+    o = O.Oracle(J, K, L, literal_r8=False, nthreads=cores)
+    for _ in range(args.warmup):
+        o.solve(rho)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.solve(rho)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = args.steps / total
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD.replace("mixed precision", "FP64 CPU restatement"),
+                       "jmax": J, "kmax": K, "lmax": L, "solves_per_step": 1, "parallelism": "openmp"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} timed solves (1 per step) of one 256x128x256 disk, "
+                                       f"SETBDY+BDYGEN+POT3, {cores} OpenMP threads, gcc -O2 "
+                                       "-ffp-contract=off"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "latency_ms": {"p50": 1e3 * float(np.median(times)),
+                           "p99": 1e3 * float(np.percentile(times, 99)), "samples": len(times)}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- CPU baseline (rank 0, N=1)
+def cpu_baseline(rhos, budget_s, max_solves):
+    """Times the oracle port on host cores over a bounded sample; returns the
+    record and its outputs (used to check the GPU results)."""
+    from oracle import oracle as O
+    cores = host_threads()
+    o = O.Oracle(J, K, L, literal_r8=False, nthreads=cores)
+    outs, t = [], 0.0
+    for rho in rhos[:max_solves]:
+        t0 = time.perf_counter()
+        phi = o.solve(rho)
+        t += time.perf_counter() - t0
+        outs.append(np.array(phi))
+        if t >= budget_s and len(outs) >= 2:
+            break
+    rec = {"value": len(outs) / t, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{len(outs)} solves of the bench's first densities (256x128x256, SETBDY+BDYGEN+POT3), "
+                     f"{t:.1f} s, {cores} OpenMP threads"}
+    return rec, outs
+
+
+# ---------------------------------------------------------------- GPU arm
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=32, help="solves per step (launch sequence)")
+    ap.add_argument("--impl", default="chymera", choices=["chymera", "reference"])
+    ap.add_argument("--refine", type=int, default=1, help="mixed-precision refinement corrections")
+    ap.add_argument("--latency-samples", type=int, default=200)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import chymera_uo_b200 as chy
+
+    rank, local, ws = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    B = args.batch
+    host = densities(B, rank * B)
+    rhos = [chy.to_cuda_fortran(r) for r in host]
+    phis = [chy.fortran_zeros_cuda((J + 2, K + 2, L)) for _ in range(B)]
+    ref_phis = [chy.fortran_zeros_cuda((J + 2, K + 2, L)) for _ in range(B)]
+    g = chy.grid(J, K, L)
+    plan = chy.Plan(g, "mixed", B)
+    plan.set_refine(args.refine)
+    plan64 = chy.Plan(g, "fp64", B)
+    stream = torch.cuda.current_stream()
+
+    # ---- device-resident throughput (the `value`)
+    for _ in range(args.warmup):
+        plan.solve_batch(rhos, phis)
+    barrier()
+    plan.set_profiling(True)
+    launches0 = plan.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.solve_batch(rhos, phis)
+        e1.record(stream)
+        barrier()
+    gpu_launches = plan.launches - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    stage, calls = plan.stage_times()
+    plan.set_profiling(False)
+    clocks = clk.summary()
+    value = ws * B * args.steps / (ms * 1e-3)
+
+    # ---- dominant kernel: the mode solves (one launch per step)
+    mode_ms = stage["mode solves"] / max(calls, 1)
+    alg = mode_solve_bytes_per_solve() * B
+    hbm, peak_kind = peaks()
+    achieved = alg / (mode_ms * 1e-3) / 1e9
+    tps = profiled_traffic_per_solve()
+    roofline = {"bound": "hbm", "kernel": "k_mode_mixed", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                "traffic": None if tps is None else tps * B,
+                "algorithmic_bytes": alg, "launch_ms": mode_ms,
+                "stage_ms_per_step": {k: v / max(calls, 1) for k, v in stage.items()}}
+
+    # ---- plain FP64 GPU path on the same inputs (same step shape)
+    for _ in range(args.warmup):
+        plan64.solve_batch(rhos, ref_phis)
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k64 = max(3, args.steps // 2)
+    f0.record(stream)
+    for _ in range(k64):
+        plan64.solve_batch(rhos, ref_phis)
+    f1.record(stream)
+    barrier()
+    ms64 = max_over_ranks(f0.elapsed_time(f1))
+    fp64_value = ws * B * k64 / (ms64 * 1e-3)
+
+    # ---- accuracy: mixed vs the FP64 GPU path, device status words
+    _, diags = plan.solve_batch(rhos, phis, diag=True)
+    torch.cuda.synchronize()
+    errs, maxe = [], []
+    for a, b in zip(phis, ref_phis):
+        d = (a[: J + 1, : K + 1] - b[: J + 1, : K + 1])
+        errs.append(float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(b[: J + 1, : K + 1])))
+        maxe.append(float(d.abs().max() / b[: J + 1, : K + 1].abs().max()))
+    accuracy = {"rel_l2_vs_fp64_gpu_max": max(errs), "max_rel_vs_fp64_gpu": max(maxe),
+                "corr_rel_solve0": diags[0]["corr_rel"], "solves_checked": B}
+
+    # ---- single-solve latency (device-resident, one launch sequence each)
+    lat = []
+    one_r, one_p = rhos[:1], phis[:1]
+    for _ in range(3):
+        plan.solve_batch(one_r, one_p)
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.latency_samples)]
+    for i in range(args.latency_samples):
+        evs[i][0].record(stream)
+        plan.solve_batch([rhos[i % B]], [phis[i % B]])
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    lat = [a.elapsed_time(b) for a, b in evs]
+    latency = {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+               "samples": len(lat), "what": "device time of one solve (batch 1), inputs in HBM"}
+
+    # ---- end to end through the public API: pinned host RHO in, PHI out
+    pin_r = [torch.empty((L, K + 2, J + 2), dtype=torch.float64, pin_memory=True).numpy().transpose()
+             for _ in range(B)]
+    pin_p = [torch.empty((L, K + 2, J + 2), dtype=torch.float64, pin_memory=True).numpy().transpose()
+             for _ in range(B)]
+    for a, b in zip(pin_r, host):
+        a[...] = b
+    for a in pin_p:
+        a[...] = 0.0
+    h2d = B * 8 * ((J + 2) * (K + 2) * L + (J + 2) * L + L)
+    d2h = B * 8 * (J + 2) * (K + 2) * L
+    ke = max(3, args.steps // 4)
+    for _ in range(args.warmup):
+        plan.solve_batch(pin_r, pin_p)
+    barrier()
+    dstream = torch.cuda.default_stream()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(dstream)
+    for _ in range(ke):
+        plan.solve_batch(pin_r, pin_p)
+    h1.record(dstream)
+    barrier()
+    mse = max_over_ranks(h0.elapsed_time(h1))
+    e2e = {"value": ws * B * ke / (mse * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "steps": ke,
+           "api": "chy_solve_batch with CHY_PTR_HOST (pinned numpy buffers)"}
+    host_ok = np.array_equal(pin_p[0], phis[0].cpu().numpy())
+    accuracy["host_path_equals_device_path"] = bool(host_ok)
+
+    # ---- CPU baseline (oracle port), rank 0 at N=1 only; also checks results
+    cpu = None
+    if ws == 1 and rank == 0 and not args.no_cpu_baseline:
+        cpu, outs = cpu_baseline(host, args.cpu_seconds, 8)
+        ws_sl = (slice(0, J + 1), slice(0, K + 1))
+        got = [p.cpu().numpy() for p in phis[: len(outs)]]
+        g64 = [p.cpu().numpy() for p in ref_phis[: len(outs)]]
+        accuracy["rel_l2_mixed_vs_oracle_max"] = max(rel_l2(a[ws_sl], b[ws_sl]) for a, b in zip(got, outs))
+        accuracy["rel_l2_fp64_vs_oracle_max"] = max(rel_l2(a[ws_sl], b[ws_sl]) for a, b in zip(g64, outs))
+        accuracy["oracle_solves_compared"] = len(outs)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "mixed: f16 hi/lo tensor-core + f32 + f64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "jmax": J, "kmax": K, "lmax": L, "solves_per_step": B,
+                           "refine_corrections": args.refine, "parallelism": f"replicas x{ws}",
+                           "l2": f"inputs larger than L2 ({B} x {8 * (J + 2) * (K + 2) * L / 1e6:.0f} MB "
+                                 "RHO + PHI resident)"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
+                "clocks": clocks, "latency_ms": latency,
+                "fp64_gpu": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms64 / k64,
+                             "mixed_over_fp64": value / fp64_value},
+                "accuracy": accuracy}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

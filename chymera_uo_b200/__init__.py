@@ -186,6 +186,8 @@ class Plan:
         ms = (C.c_double * 8)()
         calls = C.c_longlong(0)
         n = lib().chy_plan_stage_times(self._p, ms, 8, C.byref(calls))
+        if n < 0:
+            _check(-n)
         return {STAGES[i]: ms[i] for i in range(n)}, calls.value
 
     def debug_work(self, name: str, count: int) -> np.ndarray:

@@ -99,12 +99,20 @@ int chy_last_cuda_error(void) { return g_last_cuda; }
 void chy_plan_destroy(chy_plan *p)
 {
     if (!p) return;
-    for (auto &e : p->ev)
-        if (e) cudaEventDestroy(e);
+    for (auto &set : p->ev)
+        for (auto &e : set)
+            if (e) cudaEventDestroy(e);
     cudaFree(p->d_tables);
     cudaFree(p->d_work);
-    cudaFree(p->stage_rho);
-    cudaFree(p->stage_phi);
+    cudaFree(p->stage);
+    for (int i = 0; i < chy_plan::kStageSlots; i++) {
+        if (p->ev_in[i]) cudaEventDestroy(p->ev_in[i]);
+        if (p->ev_done[i]) cudaEventDestroy(p->ev_done[i]);
+        if (p->ev_out[i]) cudaEventDestroy(p->ev_out[i]);
+    }
+    if (p->ev_start) cudaEventDestroy(p->ev_start);
+    if (p->s_h2d) cudaStreamDestroy(p->s_h2d);
+    if (p->s_d2h) cudaStreamDestroy(p->s_d2h);
     cudaFreeHost(p->h_diag);
     chy_mixed_release(p);
     delete p;
@@ -231,7 +239,6 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     CHY_CUDA(cudaMemset(p->d_work, 0, p->work_bytes));
     p->nvol = (size_t)(hp.J + 2) * (hp.K + 2) * hp.L;
     CHY_CUDA(cudaMallocHost(&p->h_diag, sizeof(double) * 4 * max_batch));
-    for (auto &e : p->ev) CHY_CUDA(cudaEventCreate(&e));
     *out = p;
     return CHY_OK;
 }
@@ -253,7 +260,7 @@ int chy_plan_set_refine(chy_plan *p, int corrections)
 long long chy_plan_device_bytes(const chy_plan *p)
 {
     if (!p) return 0;
-    return (long long)(p->table_bytes + p->work_bytes);
+    return (long long)(p->table_bytes + p->work_bytes + p->stage_bytes);
 }
 
 long long chy_plan_bytes_per_solve(const chy_plan *p)
@@ -264,18 +271,38 @@ long long chy_plan_bytes_per_solve(const chy_plan *p)
     return (long long)(per * sizeof(double));
 }
 
-int chy_plan_set_profiling(chy_plan *p, int on)
+// Folds the recorded event sets into stage_ms (waits for the last one).
+static int drain_stage_events(chy_plan *p)
 {
-    if (!p) return fail(CHY_ERR_ARG, "null plan");
-    p->profile = on != 0;
-    for (double &v : p->stage_ms) v = 0.0;
-    p->stage_calls = 0;
+    for (size_t c = 0; c < p->ev_used; c++) {
+        auto &set = p->ev[c];
+        CHY_CUDA(cudaEventSynchronize(set[ST_NSTAGE]));
+        for (int i = 0; i < ST_NSTAGE; i++) {
+            float ms = 0.f;
+            CHY_CUDA(cudaEventElapsedTime(&ms, set[i], set[i + 1]));
+            p->stage_ms[i] += ms;
+        }
+        p->stage_calls++;
+    }
+    p->ev_used = 0;
     return CHY_OK;
 }
 
-int chy_plan_stage_times(const chy_plan *p, double *ms, int n, long long *calls)
+int chy_plan_set_profiling(chy_plan *p, int on)
+{
+    if (!p) return fail(CHY_ERR_ARG, "null plan");
+    const int st = drain_stage_events(p);
+    p->profile = on != 0;
+    for (double &v : p->stage_ms) v = 0.0;
+    p->stage_calls = 0;
+    return st;
+}
+
+int chy_plan_stage_times(chy_plan *p, double *ms, int n, long long *calls)
 {
     if (!p || !ms) return fail(CHY_ERR_ARG, "null argument");
+    const int st = drain_stage_events(p);
+    if (st != CHY_OK) return -st;
     for (int i = 0; i < n && i < ST_NSTAGE; i++) ms[i] = p->stage_ms[i];
     if (calls) *calls = p->stage_calls;
     return ST_NSTAGE;
@@ -285,12 +312,28 @@ long long chy_plan_launch_count(const chy_plan *p) { return p ? p->launches : 0;
 
 }  // extern "C"
 
+// Event sets kept before older ones are folded in (with a host wait).
+static constexpr size_t kMaxEventSets = 4096;
+
 // One launch sequence over nb solves whose caller buffers are in bp.
 static int run_batch(chy_plan *p, const BatchPtrs &bp, int nb, cudaStream_t s)
 {
     const DevTables &t = p->t;
     const bool prof = p->profile;
-    auto mark = [&](int i) -> cudaError_t { return prof ? cudaEventRecord(p->ev[i], s) : cudaSuccess; };
+    cudaEvent_t *evs = nullptr;
+    if (prof) {
+        if (p->ev_used == kMaxEventSets) {
+            const int st = drain_stage_events(p);
+            if (st != CHY_OK) return st;
+        }
+        if (p->ev_used == p->ev.size()) {
+            p->ev.emplace_back();
+            for (auto &e : p->ev.back()) e = nullptr;
+            for (auto &e : p->ev.back()) CHY_CUDA(cudaEventCreate(&e));
+        }
+        evs = p->ev[p->ev_used++].data();
+    }
+    auto mark = [&](int i) -> cudaError_t { return prof ? cudaEventRecord(evs[i], s) : cudaSuccess; };
     CHY_CUDA(mark(0));
     CHY_CUDA(launch_forward(t, bp, p->w, nb, s));
     CHY_CUDA(mark(1));
@@ -310,15 +353,6 @@ static int run_batch(chy_plan *p, const BatchPtrs &bp, int nb, cudaStream_t s)
     CHY_CUDA(launch_inverse(t, bp, p->w, nb, s));
     CHY_CUDA(mark(5));
     p->launches += 1 + 2 + 1 + nl + 2;
-    if (prof) {
-        CHY_CUDA(cudaEventSynchronize(p->ev[ST_NSTAGE]));
-        for (int i = 0; i < ST_NSTAGE; i++) {
-            float ms = 0.f;
-            CHY_CUDA(cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]));
-            p->stage_ms[i] += ms;
-        }
-        p->stage_calls++;
-    }
     return CHY_OK;
 }
 
@@ -339,13 +373,37 @@ static int fetch_diag(chy_plan *p, chy_diag *diag, int nb, int first, cudaStream
     return CHY_OK;
 }
 
+// Device staging slots and copy streams for host-pointer solves (first use).
+static int ensure_host_staging(chy_plan *p)
+{
+    if (p->stage) return CHY_OK;
+    const int c = std::max(1, std::min(std::min(p->max_batch, 4), kMaxBatchPtrs));
+    const size_t bytes = (size_t)chy_plan::kStageSlots * c * 2 * p->nvol * sizeof(double);
+    if (cudaMalloc(&p->stage, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        p->stage = nullptr;
+        return fail(CHY_ERR_NOMEM, "host staging slots");
+    }
+    p->stage_bytes = bytes;
+    p->stage_chunk = c;
+    CHY_CUDA(cudaStreamCreateWithFlags(&p->s_h2d, cudaStreamNonBlocking));
+    CHY_CUDA(cudaStreamCreateWithFlags(&p->s_d2h, cudaStreamNonBlocking));
+    CHY_CUDA(cudaEventCreateWithFlags(&p->ev_start, cudaEventDisableTiming));
+    for (int i = 0; i < chy_plan::kStageSlots; i++) {
+        CHY_CUDA(cudaEventCreateWithFlags(&p->ev_in[i], cudaEventDisableTiming));
+        CHY_CUDA(cudaEventCreateWithFlags(&p->ev_done[i], cudaEventDisableTiming));
+        CHY_CUDA(cudaEventCreateWithFlags(&p->ev_out[i], cudaEventDisableTiming));
+    }
+    return CHY_OK;
+}
+
 extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, double *const *phi,
                                chy_diag *diag, int ptr_kind, void *stream)
 {
     if (!p || n < 0 || (n > 0 && (!rho || !phi))) return fail(CHY_ERR_ARG, "null plan or buffers");
     cudaStream_t s = (cudaStream_t)stream;
     const HostPlan &hp = p->hp;
-    const size_t J2 = hp.J + 2, K2 = hp.K + 2, L = hp.L, bytes = p->nvol * sizeof(double);
+    const size_t J2 = hp.J + 2, K2 = hp.K + 2, L = hp.L;
     for (int i = 0; i < n; i++)
         if (!rho[i] || !phi[i]) return fail(CHY_ERR_ARG, "null rho/phi pointer");
     if (ptr_kind == CHY_PTR_DEVICE) {
@@ -362,29 +420,54 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         return CHY_OK;
     }
     if (ptr_kind != CHY_PTR_HOST) return fail(CHY_ERR_ARG, "ptr_kind");
-    // host buffers: stage through device copies, one solve at a time
-    if (!p->stage_rho) {
-        CHY_CUDA(cudaMalloc(&p->stage_rho, bytes));
-        CHY_CUDA(cudaMalloc(&p->stage_phi, bytes));
-    }
-    for (int i = 0; i < n; i++) {
-        CHY_CUDA(cudaMemcpyAsync(p->stage_rho, rho[i], bytes, cudaMemcpyHostToDevice, s));
-        // cells the solve never writes keep the caller's values:
-        // PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :)
-        CHY_CUDA(cudaMemcpy2DAsync(p->stage_phi + J2 * (K2 - 1), J2 * K2 * sizeof(double),
-                                   phi[i] + J2 * (K2 - 1), J2 * K2 * sizeof(double), J2 * sizeof(double),
-                                   L, cudaMemcpyHostToDevice, s));
-        CHY_CUDA(cudaMemcpy2DAsync(p->stage_phi + (J2 - 1), J2 * K2 * sizeof(double), phi[i] + (J2 - 1),
-                                   J2 * K2 * sizeof(double), sizeof(double), L, cudaMemcpyHostToDevice, s));
+    if (n == 0) return CHY_OK;
+    int st = ensure_host_staging(p);
+    if (st != CHY_OK) return st;
+    // Three-stage pipeline over chunks of stage_chunk solves: copy in on
+    // s_h2d, solve on the caller's stream, copy out on s_d2h.  A slot is
+    // reused only after its previous copy out has finished.
+    const size_t vb = p->nvol * sizeof(double), plane = J2 * K2 * sizeof(double);
+    const int c = p->stage_chunk, R = chy_plan::kStageSlots;
+    bool used[chy_plan::kStageSlots] = {};
+    CHY_CUDA(cudaEventRecord(p->ev_start, s));
+    CHY_CUDA(cudaStreamWaitEvent(p->s_h2d, p->ev_start, 0));
+    for (int first = 0, chunk = 0; first < n; first += c, chunk++) {
+        const int nb = std::min(c, n - first), slot = chunk % R;
+        double *base = p->stage + (size_t)slot * c * 2 * p->nvol;
+        if (used[slot]) CHY_CUDA(cudaStreamWaitEvent(p->s_h2d, p->ev_out[slot], 0));
         BatchPtrs bp{};
-        bp.rho[0] = p->stage_rho;
-        bp.phi[0] = p->stage_phi;
-        int st = run_batch(p, bp, 1, s);
+        for (int i = 0; i < nb; i++) {
+            double *dr = base + (size_t)i * 2 * p->nvol, *df = dr + p->nvol;
+            const double *hr = rho[first + i];
+            const double *hf = phi[first + i];
+            CHY_CUDA(cudaMemcpyAsync(dr, hr, vb, cudaMemcpyHostToDevice, p->s_h2d));
+            // cells the solve never writes keep the caller's values:
+            // PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :)
+            CHY_CUDA(cudaMemcpy2DAsync(df + J2 * (K2 - 1), plane, hf + J2 * (K2 - 1), plane, J2 * sizeof(double),
+                                       L, cudaMemcpyHostToDevice, p->s_h2d));
+            CHY_CUDA(cudaMemcpy2DAsync(df + (J2 - 1), plane, hf + (J2 - 1), plane, sizeof(double), L,
+                                       cudaMemcpyHostToDevice, p->s_h2d));
+            bp.rho[i] = dr;
+            bp.phi[i] = df;
+        }
+        CHY_CUDA(cudaEventRecord(p->ev_in[slot], p->s_h2d));
+        CHY_CUDA(cudaStreamWaitEvent(s, p->ev_in[slot], 0));
+        st = run_batch(p, bp, nb, s);
         if (st != CHY_OK) return st;
-        CHY_CUDA(cudaMemcpyAsync(phi[i], p->stage_phi, bytes, cudaMemcpyDeviceToHost, s));
-        st = fetch_diag(p, diag, 1, i, s);
-        if (st != CHY_OK) return st;
+        if (diag) {
+            // diagnostics are read per chunk: this synchronises the pipeline
+            st = fetch_diag(p, diag, nb, first, s);
+            if (st != CHY_OK) return st;
+        }
+        CHY_CUDA(cudaEventRecord(p->ev_done[slot], s));
+        CHY_CUDA(cudaStreamWaitEvent(p->s_d2h, p->ev_done[slot], 0));
+        for (int i = 0; i < nb; i++)
+            CHY_CUDA(cudaMemcpyAsync(phi[first + i], bp.phi[i], vb, cudaMemcpyDeviceToHost, p->s_d2h));
+        CHY_CUDA(cudaEventRecord(p->ev_out[slot], p->s_d2h));
+        used[slot] = true;
     }
+    for (int i = 0; i < R; i++)
+        if (used[i]) CHY_CUDA(cudaStreamWaitEvent(s, p->ev_out[i], 0));
     CHY_CUDA(cudaStreamSynchronize(s));
     return CHY_OK;
 }

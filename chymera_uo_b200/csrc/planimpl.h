@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <vector>
 
 #include "chy_pot3.h"
@@ -26,10 +27,22 @@ struct chy_plan {
     size_t work_bytes = 0;
     chy::Work w{};
     size_t nvol = 0;
-    double *stage_rho = nullptr, *stage_phi = nullptr;
+    // Host-pointer solves are staged through kStageSlots device slots of
+    // stage_chunk solves each (RHO and PHI per solve), so the copy in of one
+    // chunk, the solves of the next and the copy out of a third overlap.
+    static constexpr int kStageSlots = 3;
+    double *stage = nullptr;            // [slot][chunk][rho | phi] volumes
+    size_t stage_bytes = 0;
+    int stage_chunk = 0;
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+    cudaEvent_t ev_start = nullptr;
+    cudaEvent_t ev_in[kStageSlots] = {}, ev_done[kStageSlots] = {}, ev_out[kStageSlots] = {};
     double *h_diag = nullptr;   // pinned
     bool profile = false;
-    cudaEvent_t ev[ST_NSTAGE + 1] = {};
+    // One event set per profiled launch sequence, read back lazily (after
+    // the caller has synchronised) so profiling adds no host waits.
+    std::vector<std::array<cudaEvent_t, ST_NSTAGE + 1>> ev;
+    size_t ev_used = 0;
     double stage_ms[ST_NSTAGE] = {};
     long long stage_calls = 0;
     long long launches = 0;

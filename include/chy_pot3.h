@@ -126,11 +126,14 @@ int chy_last_cuda_error(void);
 /* Per-stage device timing with CUDA events recorded on the solve stream:
  * stage 0 forward transform + ring moments, 1 boundary mass integrals,
  * 2 boundary potentials + their transform, 3 mode solves, 4 inverse
- * transform + ghosts + ZAXPHI.  Enabling it synchronises after each batch. */
+ * transform + ghosts + ZAXPHI.  Recording adds no host waits; the events are
+ * read when chy_plan_stage_times is called (or every 4096 launch
+ * sequences).  Switching profiling on or off resets the totals. */
 int chy_plan_set_profiling(chy_plan *p, int on);
-/* Accumulated milliseconds per stage (n >= 5) and the number of timed
- * launch sequences; returns the number of stages. */
-int chy_plan_stage_times(const chy_plan *p, double *ms, int n, long long *calls);
+/* Waits for the recorded events, then returns the accumulated milliseconds
+ * per stage (n >= 5) and the number of timed launch sequences; returns the
+ * number of stages, or a negative CHY_* status. */
+int chy_plan_stage_times(chy_plan *p, double *ms, int n, long long *calls);
 /* Kernel launches this plan has issued so far. */
 long long chy_plan_launch_count(const chy_plan *p);
 
