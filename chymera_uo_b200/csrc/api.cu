@@ -133,7 +133,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     }
     if (precision == CHY_PREC_MIXED && !chy_mixed_supported(&p->hp)) {
         delete p;
-        return fail(CHY_ERR_UNSUPPORTED, "mixed precision needs KMAX <= 128");
+        return fail(CHY_ERR_UNSUPPORTED, "mixed precision needs KMAX <= 128 and JMAX a multiple of 16 in 64..256");
     }
     p->precision = precision;
     p->max_batch = max_batch;
@@ -217,23 +217,27 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     w.sscan = (nsub + 1) * 2 * hp.ncol;
     w.sphac = (size_t)hp.K + 2;
     w.sdiag = 4;
-    size_t per = w.sX + w.sW + w.sC + w.smom + w.ssub + w.sscan + w.sphac + w.sdiag;
+    // every array starts on a 256-byte boundary (16-byte async copies read them)
+    auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };
+    const size_t per = al(w.sX * max_batch) + al(w.sW * max_batch) + al(w.sC * max_batch) +
+                       al(w.smom * max_batch) + al(w.ssub * max_batch) + al(w.sscan * max_batch) +
+                       al(w.sphac * max_batch) + al(w.sdiag * max_batch);
     size_t ext = chy_mixed_work_doubles(p);
-    p->work_bytes = (per * max_batch + ext) * sizeof(double) + 4096;
+    p->work_bytes = (per + ext) * sizeof(double) + 4096;
     ce = cudaMalloc(&p->d_work, p->work_bytes);
     if (ce != cudaSuccess) {
         chy_plan_destroy(p);
         return fail(CHY_ERR_NOMEM, "work space");
     }
     double *q = (double *)p->d_work;
-    w.X = q; q += w.sX * max_batch;
-    w.W = q; q += w.sW * max_batch;
-    w.C = q; q += w.sC * max_batch;
-    w.mom = q; q += w.smom * max_batch;
-    w.sub = q; q += w.ssub * max_batch;
-    w.scan = q; q += w.sscan * max_batch;
-    w.phac = q; q += w.sphac * max_batch;
-    w.diag = q; q += w.sdiag * max_batch;
+    w.X = q; q += al(w.sX * max_batch);
+    w.W = q; q += al(w.sW * max_batch);
+    w.C = q; q += al(w.sC * max_batch);
+    w.mom = q; q += al(w.smom * max_batch);
+    w.sub = q; q += al(w.ssub * max_batch);
+    w.scan = q; q += al(w.sscan * max_batch);
+    w.phac = q; q += al(w.sphac * max_batch);
+    w.diag = q; q += al(w.sdiag * max_batch);
     w.coef = nullptr;
     chy_mixed_bind_work(p, q);
     CHY_CUDA(cudaMemset(p->d_work, 0, p->work_bytes));

@@ -39,6 +39,19 @@ constexpr int kMaxN = 256;          // MMA N extent (radial index, padded)
 constexpr int kAImg = 2 * kTiles * kTiles * 2;   // hi + lo FP16 tile bytes (64 KB)
 constexpr float kAScale = 4096.0f;  // eigenbasis tiles are stored times 2^12
 constexpr long long kSpinLimit = 1ll << 26;
+// residual staging: chunk width, row strides (doubles) and buffer sizes
+constexpr int kRC = 16;
+constexpr int kResYS = 18, kResXS = 22;
+constexpr int kResY = 128 * kResYS, kResBuf = kResY + 130 * kResXS;
+// epilogue staging: sD [128][33] then two [128][32] prefetch buffers
+constexpr int kEpiD = 128 * 33;
+// resident-iterate residual: three-deep ring of 32-column chunks, row stride 34
+constexpr int kRingC = 32, kRingS = 34, kRingBuf = 128 * kRingS;
+constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t kStageBytes =
+    cmax(cmax((size_t)(kEpiD + 2 * 128 * 32) * 8, (size_t)2 * kResBuf * 8), (size_t)3 * kRingBuf * 8);
+static_assert((kRingBuf * 8) % 16 == 0, "16-byte staging");
+static_assert((kEpiD * 8) % 16 == 0 && (kResY * 8) % 16 == 0 && (kResBuf * 8) % 16 == 0, "16-byte staging");
 
 // Byte offset of element (row r, k) in a K-major, 128-byte-swizzled FP16
 // operand tile with R rows and K = 128 (two 64-element row chunks).  Chunk c
@@ -157,22 +170,6 @@ __device__ __forceinline__ void tm_ld32(uint32_t taddr, float *v)
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tm_st32(uint32_t taddr, const float *v)
-{
-    uint32_t r[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) r[i] = __float_as_uint(v[i]);
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
-        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
-        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
-        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]),
-        "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]),
-        "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
-        : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-
 __device__ __forceinline__ void tm_ld16(uint32_t taddr, float *v)
 {
     uint32_t r[16];
@@ -186,19 +183,78 @@ __device__ __forceinline__ void tm_ld16(uint32_t taddr, float *v)
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tm_st16(uint32_t taddr, const float *v)
+__device__ __forceinline__ void tm_st8(uint32_t taddr, const float *v)
 {
-    uint32_t r[16];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) r[i] = __float_as_uint(v[i]);
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+                 "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                 "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+                 "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Stores without the wait: the source registers are consumed at issue;
+// tm_wait_st() before another thread or the tensor core reads the columns.
+__device__ __forceinline__ void tm_st16_nw(uint32_t taddr, const float *v)
+{
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
             taddr),
-        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
-        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
+        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
         : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
+
+__device__ __forceinline__ void tm_st32_nw(uint32_t taddr, const float *v)
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
+        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]),
+        "f"(v[17]), "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]),
+        "f"(v[25]), "f"(v[26]), "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
+        : "memory");
+}
+
+// Loads without the wait; the values are valid after tm_wait_ld18 names them
+// (as read-write operands, so no use can be scheduled before the wait).
+__device__ __forceinline__ void tm_ld16_nw(uint32_t taddr, float *v)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
+          "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
+        : "r"(taddr)
+        : "memory");
+}
+
+__device__ __forceinline__ void tm_ld1_nw(uint32_t taddr, float &v)
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=f"(v) : "r"(taddr) : "memory");
+}
+
+__device__ __forceinline__ void tm_wait_ld18(float *v, float &a, float &b)
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]),
+                   "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]),
+                   "+f"(v[15]), "+f"(a), "+f"(b)
+                 :
+                 : "memory");
+}
+
+// 16-byte global -> shared copy; bytes = 0 fills the destination with zeros
+// (src must still be a valid address)
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ float warp_max(float v)
 {
@@ -260,17 +316,24 @@ __device__ __forceinline__ void gemm_issue(uint32_t tmem, const uint8_t *sA, con
 // ---------------------------------------------------------------------------
 // The fused per-mode solver
 // ---------------------------------------------------------------------------
-// Shared memory: A tile (64 KB: hi, lo), B tile (ntile*512 B: hi, lo),
-// FP64 stencil rows, FP32 sweep coefficients, reduction scratch, barriers.
+// Shared memory: A tile (64 KB: hi, lo), the B region (B tile; between the
+// products it stages residual and update rows or holds the sweep
+// multipliers), then FP64 stencil rows, FP32 sweep coefficients, reduction
+// and exchange scratch, barriers.
 struct MixedSmem {
     static constexpr size_t a = 0;
     static constexpr size_t b = kAImg;
-    // the B region doubles as the residual/update staging area (>= 72 KB)
-    __host__ __device__ static size_t breg(int nt) { return (size_t)nt * 512 > 73728 ? (size_t)nt * 512 : 73728; }
+    __host__ __device__ static size_t breg(int nt) { return (size_t)nt * 512 > kStageBytes ? (size_t)nt * 512 : kStageBytes; }
     __host__ __device__ static size_t tables(int nt) { return b + breg(nt); }
     __host__ __device__ static size_t bytes(int nt) { return tables(nt) + 22 * 1024; }
 };
 
+// kRes: at most two approximate solves.  The first solution x0 is an FP32
+// accumulator times a power of two, so it stays exactly in tensor memory
+// columns [0, NT) and the correction works in columns [256, 256 + NT); the
+// FP64 iterate never goes through global memory.  Otherwise (more
+// corrections) the iterate is kept in FP64 in x.xbuf.
+template <bool kRes>
 __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, MixedDev x, int nb)
 {
     extern __shared__ __align__(1024) uint8_t sm[];
@@ -281,12 +344,13 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     double *d_am = reinterpret_cast<double *>(sm + MixedSmem::tables(NT));   // [256]
     double *d_cm = d_am + 256, *d_bm = d_cm + 256;                             // [256] each
     double *d_an = d_bm + 256, *d_bn = d_an + 128, *d_cn = d_bn + 128;         // [128] each
-    float *f_am = reinterpret_cast<float *>(d_cn + 128), *f_cm = f_am + 256, *f_bm = f_cm + 256;
-    float *f_lam = f_bm + 256;                                                 // [128]
+    float4 *f_t = reinterpret_cast<float4 *>(d_cn + 128);                     // [256] {g, a, c, 0}
+    float *f_lam = reinterpret_cast<float *>(f_t + 256);                       // [128]
     float *f_red = f_lam + 128;                                                // [8]
-    double *d_red = reinterpret_cast<double *>(f_red + 8);                     // [16]
-    float *f_xch = reinterpret_cast<float *>(d_red + 16);                      // [128][4]
-    uint64_t *bar_mma = reinterpret_cast<uint64_t *>(f_xch + 512);
+    double *d_red = reinterpret_cast<double *>(f_red + 8);                     // [24]
+    float *f_xch = reinterpret_cast<float *>(d_red + 24);                      // [128][4]
+    float *f_edge = f_xch + 512;                                               // [2][8][2][16]
+    uint64_t *bar_mma = reinterpret_cast<uint64_t *>(f_edge + 512);
     uint64_t *bar_a = bar_mma + 1;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_a + 1);
     int *s_flag = reinterpret_cast<int *>(tmem_slot + 1);
@@ -305,8 +369,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     for (int j = tid; j < 256; j += blockDim.x) {
         d_am[j] = j < M ? t.am[j] : 0.0;
         d_cm[j] = j < M ? t.cm[j] : 0.0;
-        f_am[j] = (float)d_am[j];
-        f_cm[j] = (float)d_cm[j];
+        f_t[j] = make_float4(0.f, (float)d_am[j], (float)d_cm[j], 0.f);
     }
     for (int k = tid; k < 128; k += blockDim.x) {
         d_an[k] = k < NZ ? t.an[k] : 0.0;
@@ -324,6 +387,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     const int NH = NT / 2;                     // columns per half (multiple of 8)
     // MMA: kind::f16, A/B FP16 K-major, D FP32, M = 128, N = NT
     const uint32_t idesc = (1u << 4) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    const int nit = kRes ? min(x.nit, 2) : x.nit;
     uint32_t ph_mma = 0, ph_a = 0;
     bool failed = false;
 
@@ -341,8 +405,19 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
         __syncthreads();
         return *s_flag == 0;
     };
-    auto issue_gemm = [&]() {
-        if (tid == 0) gemm_issue(tmem, sA, sBh, NT, idesc, bar_mma);
+    // block sums of three per-thread values into d_red[0..2] (uniform call)
+    auto block_sum3 = [&](double a, double b, double c) {
+        a = warp_sum(a);
+        b = warp_sum(b);
+        c = warp_sum(c);
+        __syncthreads();
+        if (lane == 0) { d_red[warp] = a; d_red[8 + warp] = b; d_red[16 + warp] = c; }
+        __syncthreads();
+        if (tid == 0) {
+            double sa = 0.0, sb = 0.0, sc = 0.0;
+            for (int i = 0; i < 8; ++i) { sa += d_red[i]; sb += d_red[8 + i]; sc += d_red[16 + i]; }
+            d_red[0] = sa; d_red[8] = sb; d_red[16] = sc;
+        }
     };
 
     for (long long item = blockIdx.x; item < items && !failed; item += gridDim.x) {
@@ -363,62 +438,223 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 if (j == M - 1) gm = gm - t.cmmax;
             }
             d_bm[j] = bm;
-            f_bm[j] = (float)gm;
+            f_t[j].x = (float)gm;
         }
         double *Xl = w.X + (size_t)b * w.sX + (size_t)l * K * J;
-        double *xl = x.xbuf + (size_t)b * x.sxb + (size_t)l * K * J;
+        double *xl = kRes ? nullptr : x.xbuf + (size_t)b * x.sxb + (size_t)l * K * J;
         double *cr = x.corr + (size_t)b * x.scorr + (size_t)l * 16;
+        double u0 = 0.0;   // kRes: scale of x0 held in tensor memory
         __syncthreads();
 
-        for (int it = 0; it < x.nit && !failed; ++it) {
-            const bool last = it == x.nit - 1;
+        for (int it = 0; it < nit && !failed; ++it) {
+            const bool last = it == nit - 1;
+            const bool res_x = kRes && it > 0;          // x0 read from tensor memory
+            const uint32_t acc = res_x ? 256u : 0u;     // product / sweep columns
+            double sxx = 0.0;                           // kRes: sum of x0^2
             // ---- residual r = Y - A_m x (FP64) -> TMEM cols [256, 256+NT) as FP32.
-            // Staged in 32-column chunks through the B-tile region (unused until
-            // the split below) so global rows are read coalesced: sY[k][jj]
-            // (stride 33) and the iterate with a one-cell halo (stride 35).
-            // Out-of-range neighbours are staged as 0; their stencil
-            // coefficients (AN(1), CN(KMAX-1), AM(1), CM(JMAX-1)) are 0 too.
+            // Out-of-range neighbours read as 0; their stencil coefficients
+            // (AN(1), CN(KMAX-1), AM(1), CM(JMAX-1)) are 0 too.  JMAX is a
+            // multiple of 16, so column M is in the chunk of column M-1 and
+            // every 16-byte granule of a row is aligned.
             float rmax = 0.0f;
-            {
-                double *sY = reinterpret_cast<double *>(sBh);
-                double *sXs = sY + 128 * 33;
-                for (int c0 = 0; c0 < NT; c0 += 32) {
-                    __syncthreads();
-                    for (int i = tid; i < 128 * 32; i += 256) {
-                        const int k = i >> 5, jj = i & 31, j = c0 + jj;
-                        double y = 0.0;
-                        if (j < M && k < NZ) {
-                            y = t.pig4 * Xl[(size_t)k * J + j];
-                            if (k == NZ - 1) y = y - t.cnmax * Xl[(size_t)NZ * J + j];
-                            if (j == M - 1) y = y - t.cmmax * Xl[(size_t)k * J + M];
-                        }
-                        sY[k * 33 + jj] = y;
-                    }
-                    if (it > 0) {
-                        for (int i = tid; i < 130 * 34; i += 256) {
-                            const int kk = i / 34 - 1, jj = i % 34 - 1, j = c0 + jj;
-                            sXs[(kk + 1) * 35 + (jj + 1)] =
-                                (kk >= 0 && kk < NZ && j >= 0 && j < M) ? xl[(size_t)kk * J + j] : 0.0;
+            if constexpr (kRes) {
+                // Raw X rows k = 0..KMAX-1 (boundary row NZ and column M
+                // included) stream through a three-deep cp.async ring of
+                // 32-column chunks; x0 comes from tensor memory, its vertical
+                // neighbours by warp shuffles and, across warps, through
+                // shared memory.  Row stride 17 granules: the 16-byte reads of
+                // eight consecutive rows fall on distinct banks.
+                double *ring = reinterpret_cast<double *>(sBh);
+                const int nchr = NT / kRingC;
+                auto issue = [&](int c) {
+                    if (c < nchr) {
+                        double *sy = ring + (c % 3) * kRingBuf;
+                        const int c0 = c * kRingC;
+                        for (int g = tid; g < K * (kRingC / 2); g += 256) {
+                            const int k = g >> 4, q = g & 15, j = c0 + 2 * q;
+                            const bool ok = j < J;
+                            cp_async16(sy + k * kRingS + 2 * q, ok ? Xl + (size_t)k * J + j : Xl, ok ? 16 : 0);
                         }
                     }
-                    __syncthreads();
-                    float v[16];
-                    const int k = kq, jb = jh * 16;
+                    cp_async_commit();
+                };
+                issue(0);
+                issue(1);
+                const int k = kq, jb = jh * 16, quad = warp & 3;
+                const bool krow = k < NZ;
+                const double an = d_an[k], cn = d_cn[k], bnk = d_bn[k];
+                for (int c = 0; c < nchr; ++c) {
+                    const int c0 = c * kRingC;
+                    float xc[16], xlf = 0.f, xrt = 0.f;
+                    if (res_x) {
+                        const int jl = c0 + jb - 1, jr = c0 + jb + 16;
+                        tm_ld16_nw(tmem + lane_base + c0 + jb, xc);
+                        tm_ld1_nw(tmem + lane_base + (uint32_t)(jl < 0 ? 0 : jl), xlf);
+                        tm_ld1_nw(tmem + lane_base + (uint32_t)(jr < NT ? jr : NT - 1), xrt);
+                        tm_wait_ld18(xc, xlf, xrt);
+                        if (jl < 0) xlf = 0.f;
+                        if (jr >= NT) xrt = 0.f;
+                        float *ed = f_edge + ((c & 1) * 8 + warp) * 32;
+                        if (lane == 0) {
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) {
+                            for (int u = 0; u < 16; ++u) ed[u] = xc[u];
+                        }
+                        if (lane == 31) {
+#pragma unroll
+                            for (int u = 0; u < 16; ++u) ed[16 + u] = xc[u];
+                        }
+                    }
+                    cp_async_wait<1>();
+                    __syncthreads();
+                    issue(c + 2);
+                    // branch-free: the folds are multiplied by zero where they do
+                    // not apply, cells outside the interior are selected away
+                    const double *buf = ring + (c % 3) * kRingBuf;
+                    const double *sy = buf + k * kRingS;
+                    double yv[16], yt[16];
+#pragma unroll
+                    for (int u = 0; u < 16; u += 2) {
+                        const double2 t2 = *reinterpret_cast<const double2 *>(sy + jb + u);
+                        const double2 t3 = *reinterpret_cast<const double2 *>(buf + NZ * kRingS + jb + u);
+                        yv[u] = t2.x;
+                        yv[u + 1] = t2.y;
+                        yt[u] = t3.x;
+                        yt[u + 1] = t3.y;
+                    }
+                    const double ytop = k == NZ - 1 ? t.cnmax : 0.0;
+                    const double yM = sy[max(min(M - c0, kRingC - 1), 0)];
+                    float v[16];
+                    if (res_x) {
+                        const float *eu = f_edge + ((c & 1) * 8 + warp - 1) * 32 + 16;   // row above lane 0
+                        const float *ed = f_edge + ((c & 1) * 8 + warp + 1) * 32;        // row below lane 31
+                        double xd_[18];   // x0 at columns j-1 .. j+16 (unscaled)
+                        xd_[0] = (double)xlf;
+                        xd_[17] = (double)xrt;
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) xd_[u + 1] = (double)xc[u];
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) {
+                            const int j = c0 + jb + u;
+                            float xu = __shfl_up_sync(0xffffffffu, xc[u], 1);
+                            float xd = __shfl_down_sync(0xffffffffu, xc[u], 1);
+                            if (lane == 0) xu = quad > 0 ? eu[u] : 0.f;
+                            if (lane == 31) xd = quad < 3 ? ed[u] : 0.f;
+                            // A x0 / u0: u0 is a power of two, so scaling the sum is exact
+                            double ax = (bnk + d_bm[j]) * xd_[u + 1];
+                            ax = fma(an, (double)xu, ax);
+                            ax = fma(cn, (double)xd, ax);
+                            ax = fma(d_am[j], xd_[u], ax);
+                            ax = fma(d_cm[j], xd_[u + 2], ax);
+                            double r = t.pig4 * yv[u];
+                            r = fma(-ytop, yt[u], r);
+                            r = fma(j == M - 1 ? -t.cmmax : 0.0, yM, r);
+                            r = fma(-u0, ax, r);
+                            const bool in = krow && j < M;
+                            sxx = fma(in ? xd_[u + 1] : 0.0, xd_[u + 1], sxx);
+                            v[u] = in ? (float)r : 0.f;
+                            rmax = fmaxf(rmax, fabsf(v[u]));
+                        }
+                    } else {
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) {
+                            const int j = c0 + jb + u;
+                            double r = t.pig4 * yv[u];
+                            r = fma(-ytop, yt[u], r);
+                            r = fma(j == M - 1 ? -t.cmmax : 0.0, yM, r);
+                            v[u] = (krow && j < M) ? (float)r : 0.f;
+                            rmax = fmaxf(rmax, fabsf(v[u]));
+                        }
+                    }
+                    tm_st16_nw(tmem + lane_base + 256 + c0 + jb, v);
+                }
+                cp_async_wait<0>();
+                tm_wait_st();
+            } else {
+                // Chunks of kRC columns, double-buffered with cp.async: raw X
+                // rows k = 0..KMAX-1 and the iterate rows k = -1..NZ with
+                // columns c0-2 .. c0+kRC+1 (out-of-range granules are zero).
+                // Row strides of 9 and 11 granules keep the 16-byte reads of
+                // eight consecutive rows on distinct banks.
+                double *stage = reinterpret_cast<double *>(sBh);
+                const bool need_x = it > 0;
+                auto issue = [&](int c0, int buf) {
+                    double *sy = stage + buf * kResBuf, *sx = sy + kResY;
+                    for (int g = tid; g < K * (kRC / 2); g += 256) {
+                        const int k = g / (kRC / 2), j = c0 + 2 * (g % (kRC / 2));
+                        const bool ok = j < J;
+                        cp_async16(sy + k * kResYS + (j - c0), ok ? Xl + (size_t)k * J + j : Xl, ok ? 16 : 0);
+                    }
+                    if (need_x) {
+                        for (int g = tid; g < (NZ + 2) * (kRC / 2 + 2); g += 256) {
+                            const int kk = g / (kRC / 2 + 2) - 1, j = c0 - 2 + 2 * (g % (kRC / 2 + 2));
+                            const bool ok = kk >= 0 && kk < NZ && j >= 0 && j < J;
+                            cp_async16(sx + (kk + 1) * kResXS + (j - c0 + 2), ok ? xl + (size_t)kk * J + j : xl,
+                                       ok ? 16 : 0);
+                        }
+                    }
+                    cp_async_commit();
+                };
+                const int nch = NT / kRC;
+                issue(0, 0);
+                const int k = kq, jb = jh * (kRC / 2);
+                const bool krow = k < NZ;
+                const double an = d_an[k], cn = d_cn[k], bnk = d_bn[k];
+                for (int c = 0; c < nch; ++c) {
+                    const int c0 = c * kRC;
+                    if (c + 1 < nch) {
+                        issue(c0 + kRC, (c + 1) & 1);
+                        cp_async_wait<1>();
+                    } else {
+                        cp_async_wait<0>();
+                    }
+                    __syncthreads();
+                    const double *sy = stage + (c & 1) * kResBuf, *sx = sy + kResY;
+                    float v[kRC / 2];
+                    double yv[kRC / 2], xc[kRC / 2 + 4], xu[kRC / 2], xd[kRC / 2];
+#pragma unroll
+                    for (int u = 0; u < kRC / 2; u += 2) {
+                        const double2 t2 = *reinterpret_cast<const double2 *>(sy + k * kResYS + jb + u);
+                        yv[u] = t2.x;
+                        yv[u + 1] = t2.y;
+                    }
+                    if (need_x) {
+#pragma unroll
+                        for (int u = 0; u < kRC / 2 + 4; u += 2) {
+                            const double2 t2 = *reinterpret_cast<const double2 *>(sx + (k + 1) * kResXS + jb + u);
+                            xc[u] = t2.x;
+                            xc[u + 1] = t2.y;
+                        }
+#pragma unroll
+                        for (int u = 0; u < kRC / 2; u += 2) {
+                            const double2 a2 = *reinterpret_cast<const double2 *>(sx + k * kResXS + jb + 2 + u);
+                            const double2 b2 = *reinterpret_cast<const double2 *>(sx + (k + 2) * kResXS + jb + 2 + u);
+                            xu[u] = a2.x;
+                            xu[u + 1] = a2.y;
+                            xd[u] = b2.x;
+                            xd[u + 1] = b2.y;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kRC / 2; ++u) {
                         const int jj = jb + u, j = c0 + jj;
-                        double r = sY[k * 33 + jj];
-                        if (it > 0 && j < M && k < NZ) {
-                            const double *xr = sXs + (k + 1) * 35 + (jj + 1);
-                            const double ax = (d_bn[k] + d_bm[j]) * xr[0] + d_an[k] * xr[-35] + d_cn[k] * xr[35] +
-                                              d_am[j] * xr[-1] + d_cm[j] * xr[1];
-                            r = r - ax;
+                        double r = 0.0;
+                        if (krow && j < M) {
+                            r = t.pig4 * yv[u];
+                            if (k == NZ - 1) r = r - t.cnmax * sy[NZ * kResYS + jj];
+                            if (j == M - 1) r = r - t.cmmax * sy[k * kResYS + (M - c0)];
+                            if (need_x) {
+                                const double ax = (bnk + d_bm[j]) * xc[u + 2] + an * xu[u] + cn * xd[u] +
+                                                  d_am[j] * xc[u + 1] + d_cm[j] * xc[u + 3];
+                                r = r - ax;
+                            }
                         }
                         v[u] = (float)r;
                         rmax = fmaxf(rmax, fabsf(v[u]));
                     }
-                    tm_st16(tmem + lane_base + 256 + c0 + jb, v);
+                    tm_st8(tmem + lane_base + 256 + c0 + jb, v);
+                    __syncthreads();
                 }
+                tm_wait_st();
             }
             rmax = warp_max(rmax);
             if (lane == 0) f_red[warp] = rmax;
@@ -438,10 +674,10 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             fence_proxy_async();
             tc_fence_before();
             __syncthreads();
-            // ---- W = U r (vertical transform) into TMEM cols [0, NT)
+            // ---- W = U r (vertical transform) into TMEM cols [acc, acc + NT)
             if (a_inflight && !wait_all(bar_a, ph_a)) { failed = true; break; }
             a_inflight = false;
-            issue_gemm();
+            if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma);
             if (!wait_all(bar_mma, ph_mma)) { failed = true; break; }
             tc_fence_after();
             if (tid == 0) {   // A tile free: bring in V
@@ -449,123 +685,117 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 bulk_g2s(sA, x.aimg + kAImg, kAImg, bar_a);
             }
             a_inflight = true;
-            // ---- radial sweeps (T_r(m) + lam_p) w = W_p, top-down and bottom-up halves
+            // ---- radial sweeps (T_r(m) + lam_p) w = W_p, top-down and bottom-up
+            // halves.  The multipliers go to shared memory (the B tile is free
+            // until the next split): cvs[j][p].
             float xmax = 0.0f;
             {
+                float *cvs = reinterpret_cast<float *>(sBh);
                 const int p = kq;
                 const bool live = p < NZ;
                 const float lam = f_lam[p];
-                const int h = min(32 * ((M + 63) / 64), M);   // rows [0,h) top, [h,M) bottom
-                float yv[32], cv[32];
-                float ymid = 0.f, cmid = 0.f;
+                const int h = 32 * ((M + 63) / 64);   // rows [0,h) top, [h,M) bottom; M >= 63
+                const uint32_t tb = tmem + lane_base + acc;
+                float yv[32];
                 // Elimination in excess form: with g = d + a + c (the small
                 // diagonal excess) the top-down multipliers c' = c/D are kept as
                 // e = 1 + c' = (g - a e_prev)/D, D = (g - a e_prev) - c, so no
                 // near-cancelling sum is formed in FP32; bottom-up likewise with
                 // f = 1 + a''.
+                // The loops are branch-free (h is a multiple of 32 and h < M):
+                // rows outside [0, M) and padding lanes (p >= NZ) compute
+                // values that are discarded by selects, so the coefficient
+                // loads of a chunk can all be issued ahead of the recurrence.
+                float cv[32];
                 if (jh == 0) {
                     float e = 0.f, yp = 0.f;
                     for (int c0 = 0; c0 < h; c0 += 32) {
-                        tm_ld32(tmem + lane_base + c0, yv);
+                        tm_ld32(tb + c0, yv);
 #pragma unroll
                         for (int u = 0; u < 32; ++u) {
-                            const int j = c0 + u;
-                            if (j < h && live) {
-                                const float tt = (f_bm[j] + lam) - f_am[j] * e;
-                                const float rr = __fdividef(1.0f, tt - f_cm[j]);
-                                e = tt * rr;
-                                yp = (yv[u] - f_am[j] * yp) * rr;
-                                yv[u] = yp;
-                                cv[u] = e;
-                            } else {
-                                cv[u] = 0.f;
-                            }
+                            const float4 T = f_t[c0 + u];
+                            const float tt = (T.x + lam) - T.y * e;
+                            const float rr = __fdividef(1.0f, tt - T.z);
+                            e = tt * rr;
+                            yp = (yv[u] - T.y * yp) * rr;
+                            yv[u] = yp;
+                            cv[u] = e;
                         }
-                        tm_st32(tmem + lane_base + c0, yv);
-                        tm_st32(tmem + lane_base + 256 + c0, cv);
+                        tm_st32_nw(tb + c0, yv);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) cvs[(c0 + u) * 128 + p] = cv[u];
                     }
-                    ymid = yp;
-                    cmid = e;
-                    f_xch[p * 4 + 0] = ymid;
-                    f_xch[p * 4 + 1] = cmid;
-                } else if (h < M) {
+                    f_xch[p * 4 + 0] = yp;
+                    f_xch[p * 4 + 1] = e;
+                } else {
                     float f = 0.f, yp = 0.f;
                     const int cl = ((M - 1) / 32) * 32;
                     for (int c0 = cl; c0 >= h; c0 -= 32) {
-                        tm_ld32(tmem + lane_base + c0, yv);
+                        tm_ld32(tb + c0, yv);
 #pragma unroll
                         for (int u = 31; u >= 0; --u) {
-                            const int j = c0 + u;
-                            if (j < M && live) {
-                                const float tt = (f_bm[j] + lam) - f_cm[j] * f;
-                                const float rr = __fdividef(1.0f, tt - f_am[j]);
-                                f = tt * rr;
-                                yp = (yv[u] - f_cm[j] * yp) * rr;
-                                yv[u] = yp;
-                                cv[u] = f;
-                            } else {
-                                cv[u] = 0.f;
-                            }
+                            const bool in = c0 + u < M;   // uniform
+                            const float4 T = f_t[c0 + u];
+                            const float tt = (T.x + lam) - T.z * f;
+                            const float rr = __fdividef(1.0f, tt - T.y);
+                            const float fn = tt * rr, yn = (yv[u] - T.z * yp) * rr;
+                            f = in ? fn : f;
+                            yp = in ? yn : yp;
+                            yv[u] = yn;
+                            cv[u] = fn;
                         }
-                        tm_st32(tmem + lane_base + c0, yv);
-                        tm_st32(tmem + lane_base + 256 + c0, cv);
+                        tm_st32_nw(tb + c0, yv);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) cvs[(c0 + u) * 128 + p] = cv[u];
                     }
                     f_xch[p * 4 + 2] = yp;
                     f_xch[p * 4 + 3] = f;
                 }
+                tm_wait_st();
                 __syncthreads();
                 // meeting rows h-1 (top) and h (bottom):
                 // x_t = y'_t + (1-e_t) x_u, x_u = y''_u + (1-f_u) x_t
                 float xt, xu;
                 {
                     const float yt = f_xch[p * 4 + 0], et = f_xch[p * 4 + 1];
-                    if (h < M) {
-                        const float yu = f_xch[p * 4 + 2], fu = f_xch[p * 4 + 3];
-                        xt = (yt + (1.0f - et) * yu) / ((et + fu) - et * fu);
-                        xu = yu + (1.0f - fu) * xt;
-                    } else {
-                        xt = yt;
-                        xu = 0.f;
-                    }
+                    const float yu = f_xch[p * 4 + 2], fu = f_xch[p * 4 + 3];
+                    xt = (yt + (1.0f - et) * yu) / ((et + fu) - et * fu);
+                    xu = yu + (1.0f - fu) * xt;
                 }
-                if (!live) { xt = 0.f; xu = 0.f; }
                 if (jh == 0) {
                     float xn = xt;   // x_{j+1} while sweeping up
-                    for (int c0 = ((h - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
-                        tm_ld32(tmem + lane_base + c0, yv);
-                        tm_ld32(tmem + lane_base + 256 + c0, cv);
+                    for (int c0 = h - 32; c0 >= 0; c0 -= 32) {
+                        tm_ld32(tb + c0, yv);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) cv[u] = cvs[(c0 + u) * 128 + p];
 #pragma unroll
                         for (int u = 31; u >= 0; --u) {
-                            const int j = c0 + u;
-                            float xv = 0.f;
-                            if (j < h && live) {
-                                xv = (j == h - 1) ? xt : yv[u] + (1.0f - cv[u]) * xn;
-                                xn = xv;
-                            }
-                            yv[u] = xv;
-                            xmax = fmaxf(xmax, fabsf(xv));
+                            float xv = yv[u] + (1.0f - cv[u]) * xn;
+                            xv = (c0 + u == h - 1) ? xt : xv;
+                            xn = xv;
+                            yv[u] = live ? xv : 0.f;
+                            xmax = fmaxf(xmax, fabsf(yv[u]));
                         }
-                        tm_st32(tmem + lane_base + c0, yv);
+                        tm_st32_nw(tb + c0, yv);
                     }
                 } else {
                     float xp = xu;   // x_{j-1} while sweeping down
-                    for (int c0 = (h / 32) * 32; c0 < NT; c0 += 32) {
-                        tm_ld32(tmem + lane_base + c0, yv);
-                        tm_ld32(tmem + lane_base + 256 + c0, cv);
+                    for (int c0 = h; c0 < NT; c0 += 32) {
+                        tm_ld32(tb + c0, yv);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) cv[u] = cvs[(c0 + u) * 128 + p];
 #pragma unroll
                         for (int u = 0; u < 32; ++u) {
-                            const int j = c0 + u;   // h is a multiple of 32: j >= h
-                            float xv = 0.f;
-                            if (j < M && live) {
-                                xv = (j == h) ? xu : yv[u] + (1.0f - cv[u]) * xp;
-                                xp = xv;
-                            }
-                            yv[u] = xv;
-                            xmax = fmaxf(xmax, fabsf(xv));
+                            float xv = yv[u] + (1.0f - cv[u]) * xp;
+                            xv = (c0 + u == h) ? xu : xv;
+                            xp = xv;
+                            yv[u] = (live && c0 + u < M) ? xv : 0.f;
+                            xmax = fmaxf(xmax, fabsf(yv[u]));
                         }
-                        tm_st32(tmem + lane_base + c0, yv);
+                        tm_st32_nw(tb + c0, yv);
                     }
                 }
+                tm_wait_st();
             }
             xmax = warp_max(xmax);
             if (lane == 0) f_red[warp] = xmax;
@@ -578,17 +808,17 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             // ---- TMEM w -> B tile (row j, K index p), FP16 hi/lo
             for (int c0 = jh * NH; c0 < (jh + 1) * NH; c0 += 32) {
                 float v[32];
-                tm_ld32(tmem + lane_base + c0, v);
+                tm_ld32(tmem + lane_base + acc + c0, v);
 #pragma unroll
                 for (int u = 0; u < 32; ++u) put_split(sBh, sBl, c0 + u, kq, NT, v[u] * s2);
             }
             fence_proxy_async();
             tc_fence_before();
             __syncthreads();
-            // ---- delta = V w into TMEM cols [0, NT)
+            // ---- delta = V w into TMEM cols [acc, acc + NT)
             if (!wait_all(bar_a, ph_a)) { failed = true; break; }
             a_inflight = false;
-            issue_gemm();
+            if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma);
             if (!wait_all(bar_mma, ph_mma)) { failed = true; break; }
             tc_fence_after();
             const bool more = !last || item + gridDim.x < items;
@@ -597,45 +827,103 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 bulk_g2s(sA, x.aimg, kAImg, bar_a);
             }
             a_inflight = more;
-            // ---- x += delta (FP64); the last pass writes the interior of X
             const double unscale = 1.0 / ((double)kAScale * (double)kAScale * (double)s1 * (double)s2);
-            // staged like the residual: TMEM rows -> sD[k][jj] -> coalesced rows
-            double sd = 0.0, sx = 0.0;
-            {
+            if constexpr (kRes) {
+                if (!last) {
+                    u0 = unscale;   // x0 stays in tensor memory columns [0, NT)
+                    continue;
+                }
+                // X = x0 + delta (FP64), staged through sD[k][jj] to write rows
                 double *sD = reinterpret_cast<double *>(sBh);
+                double sd = 0.0, sx = 0.0;
+                const int jb = jh * 16;
                 for (int c0 = 0; c0 < NT; c0 += 32) {
-                    float v[16];
-                    const int jb = jh * 16;
-                    tm_ld16(tmem + lane_base + c0 + jb, v);
+                    float dv[16], xv[16];
+                    tm_ld16(tmem + lane_base + acc + c0 + jb, dv);
+                    if (res_x) tm_ld16(tmem + lane_base + c0 + jb, xv);
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const int j = c0 + jb + u;
+                        const double dl = (double)dv[u] * unscale;
+                        const double xn = (res_x ? (double)xv[u] * u0 : 0.0) + dl;
+                        sD[kq * 33 + jb + u] = xn;
+                        if (kq < NZ && j < M) {
+                            sd += dl * dl;
+                            sx += xn * xn;
+                        }
+                    }
                     __syncthreads();
+                    for (int i = tid; i < 128 * 32; i += 256) {
+                        const int k = i >> 5, jj = i & 31, j = c0 + jj;
+                        if (k < NZ && j < M) Xl[(size_t)k * J + j] = sD[k * 33 + jj];
+                    }
+                    __syncthreads();
+                }
+                block_sum3(sd, sx, sxx);
+                if (tid == 0) {
+                    if (res_x) {   // the first solve's delta is x0 itself
+                        cr[0] = d_red[16] * u0 * u0;
+                        cr[1] = d_red[16] * u0 * u0;
+                    }
+                    cr[2 * it] = d_red[0];
+                    cr[2 * it + 1] = d_red[8];
+                }
+                __syncthreads();
+            } else {
+                // ---- x += delta (FP64); the last pass writes the interior of X.
+                // TMEM rows -> sD[k][jj] -> coalesced rows of x; the previous
+                // iterate's rows are prefetched one chunk ahead
+                double sd = 0.0, sx = 0.0;
+                double *sD = reinterpret_cast<double *>(sBh);
+                double *sO = sD + kEpiD;
+                const bool need_x = it > 0;
+                auto issue = [&](int c0, int buf) {
+                    double *so = sO + buf * (128 * 32);
+                    for (int g = tid; g < 128 * 16; g += 256) {
+                        const int k = g >> 4, j = c0 + 2 * (g & 15);
+                        const bool ok = k < NZ && j < J;
+                        cp_async16(so + k * 32 + (j - c0), ok ? xl + (size_t)k * J + j : xl, ok ? 16 : 0);
+                    }
+                    cp_async_commit();
+                };
+                const int nch = NT / 32, jb = jh * 16;
+                if (need_x) issue(0, 0);
+                for (int c = 0; c < nch; ++c) {
+                    const int c0 = c * 32;
+                    if (need_x) {
+                        if (c + 1 < nch) {
+                            issue(c0 + 32, (c + 1) & 1);
+                            cp_async_wait<1>();
+                        } else {
+                            cp_async_wait<0>();
+                        }
+                    }
+                    float v[16];
+                    tm_ld16(tmem + lane_base + c0 + jb, v);
 #pragma unroll
                     for (int u = 0; u < 16; ++u) sD[kq * 33 + jb + u] = (double)v[u] * unscale;
                     __syncthreads();
+                    const double *so = sO + (c & 1) * (128 * 32);
                     for (int i = tid; i < 128 * 32; i += 256) {
                         const int k = i >> 5, jj = i & 31, j = c0 + jj;
                         if (k < NZ && j < M) {
                             const double dlt = sD[k * 33 + jj];
                             const size_t o = (size_t)k * J + j;
-                            const double xn = (it > 0 ? xl[o] : 0.0) + dlt;
+                            const double xn = (need_x ? so[k * 32 + jj] : 0.0) + dlt;
                             if (last) Xl[o] = xn;
                             else xl[o] = xn;
                             sd += dlt * dlt;
                             sx += xn * xn;
                         }
                     }
+                    __syncthreads();
                 }
-            }
-            sd = warp_sum(sd);
-            sx = warp_sum(sx);
-            if (lane == 0) { d_red[warp] = sd; d_red[8 + warp] = sx; }
-            tc_fence_before();
-            __syncthreads();
-            tc_fence_after();
-            if (tid == 0) {
-                double a = 0.0, c = 0.0;
-                for (int i = 0; i < 8; ++i) { a += d_red[i]; c += d_red[8 + i]; }
-                cr[2 * it] = a;
-                cr[2 * it + 1] = c;
+                block_sum3(sd, sx, 0.0);
+                if (tid == 0) {
+                    cr[2 * it] = d_red[0];
+                    cr[2 * it + 1] = d_red[8];
+                }
+                __syncthreads();
             }
         }
     }
@@ -652,7 +940,10 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
 // ---------------------------------------------------------------------------
 static int round64(int v) { return (v + 63) / 64 * 64; }
 
-bool chy_mixed_supported(const chy::HostPlan *hp) { return hp->NZ <= 127 && hp->J >= 64 && round64(hp->J) <= kMaxN; }
+bool chy_mixed_supported(const chy::HostPlan *hp)
+{
+    return hp->NZ <= 127 && hp->J >= 64 && hp->J % 16 == 0 && round64(hp->J) <= kMaxN;
+}
 
 size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image)
 {
@@ -725,12 +1016,18 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
     MixedDev d = p->mx->dev;
     d.nit = 1 + p->refine;
     if (d.nit > 8) d.nit = 8;
+    // the kernel streams X and the iterate with 16-byte async copies
+    if ((reinterpret_cast<uintptr_t>(p->w.X) | reinterpret_cast<uintptr_t>(d.xbuf)) % 16 != 0 || p->hp.J % 16 != 0)
+        return CHY_ERR_ARG;
     const size_t sm = MixedSmem::bytes(d.ntile);
-    cudaError_t e = ensure_smem((const void *)k_mode_mixed, sm);
+    // two approximate solves (one correction) keep the iterate in tensor memory
+    const void *kern = d.nit <= 2 ? (const void *)k_mode_mixed<true> : (const void *)k_mode_mixed<false>;
+    cudaError_t e = ensure_smem(kern, sm);
     if (e != cudaSuccess) return CHY_ERR_CUDA;
     const long long items = (long long)nb * p->hp.L;
     const int grid = (int)(items < p->num_sms ? items : p->num_sms);
-    k_mode_mixed<<<grid, 256, sm, s>>>(p->t, p->w, d, nb);
+    if (d.nit <= 2) k_mode_mixed<true><<<grid, 256, sm, s>>>(p->t, p->w, d, nb);
+    else k_mode_mixed<false><<<grid, 256, sm, s>>>(p->t, p->w, d, nb);
     if (cudaGetLastError() != cudaSuccess) return CHY_ERR_CUDA;
     *launches = 1;
     return CHY_OK;
