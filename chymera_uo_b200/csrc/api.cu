@@ -523,3 +523,74 @@ cudaError_t chy::ensure_smem(const void *kernel, size_t bytes)
     if (e == cudaSuccess) m[kernel] = (int)bytes;
     return e;
 }
+
+// ---------------------------------------------------------------------------
+// chy_solve_static: the FP64 device-pointer solve with its per-solve work
+// space taken from one fixed, statically sized device array instead of the
+// plan's allocation.  The call itself allocates nothing (no cudaMalloc, no
+// cudaFree, no allocating library routine).  One array per device, shared by
+// every plan: overlapping calls on the same device (from several streams or
+// threads) race on it and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+static constexpr size_t kStaticScratchBytes = (size_t)8 << 20;   // 8 MiB
+static __device__ __align__(256) double g_static_scratch[kStaticScratchBytes / sizeof(double)];
+
+namespace {
+std::mutex g_static_mu;
+double *g_static_ptr[64] = {};   // per device: address of g_static_scratch
+}  // namespace
+
+extern "C" int chy_solve_static(chy_plan *p, const double *rho, double *phi, void *stream)
+{
+    if (!p || !rho || !phi) return fail(CHY_ERR_ARG, "null plan or buffers");
+    if (p->precision != CHY_PREC_FP64) return fail(CHY_ERR_UNSUPPORTED, "chy_solve_static runs FP64 plans only");
+    // the plan's per-solve arrays, 256-byte aligned pieces, carved from the static array
+    const Work &pw = p->w;
+    auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };
+    const size_t need = al(pw.sX) + al(pw.sW) + al(pw.sC) + al(pw.smom) + al(pw.ssub) + al(pw.sscan) +
+                        al(pw.sphac) + al(pw.sdiag);
+    if (need * sizeof(double) > kStaticScratchBytes)
+        return fail(CHY_ERR_CAPACITY, "chy_solve_static: this grid needs " + std::to_string(need * sizeof(double)) +
+                                          " bytes of work space; the static scratch holds " +
+                                          std::to_string(kStaticScratchBytes) + " bytes");
+    int dev = 0;
+    CHY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(CHY_ERR_ARG, "device ordinal out of range");
+    double *base = nullptr;
+    {
+        // first call on each device (with that device current): look the
+        // array up once; later calls reuse the address
+        std::lock_guard<std::mutex> lk(g_static_mu);
+        if (!g_static_ptr[dev]) {
+            void *ptr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+            g_static_ptr[dev] = static_cast<double *>(ptr);
+        }
+        base = g_static_ptr[dev];
+    }
+    Work w = pw;   // strides
+    double *q = base;
+    w.X = q; q += al(pw.sX);
+    w.W = q; q += al(pw.sW);
+    w.C = q; q += al(pw.sC);
+    w.mom = q; q += al(pw.smom);
+    w.sub = q; q += al(pw.ssub);
+    w.scan = q; q += al(pw.sscan);
+    w.phac = q; q += al(pw.sphac);
+    w.diag = q;
+    w.coef = nullptr;   // /COEFS/ output only through chy_solve
+    cudaStream_t s = (cudaStream_t)stream;
+    // every call starts from zeroed work space, as the plan's own allocation does
+    CHY_CUDA(cudaMemsetAsync(base, 0, need * sizeof(double), s));
+    BatchPtrs bp{};
+    bp.rho[0] = rho;
+    bp.phi[0] = phi;
+    const DevTables &t = p->t;
+    CHY_CUDA(launch_forward(t, bp, w, 1, s));
+    CHY_CUDA(launch_bdy_sums(t, w, 1, s));
+    CHY_CUDA(launch_bdy_synth(t, w, 1, s));
+    CHY_CUDA(launch_solve_fp64(t, w, 1, p->num_sms, s));
+    CHY_CUDA(launch_inverse(t, bp, w, 1, s));
+    return CHY_OK;
+}

@@ -137,6 +137,24 @@ int chy_plan_stage_times(chy_plan *p, double *ms, int n, long long *calls);
 /* Kernel launches this plan has issued so far. */
 long long chy_plan_launch_count(const chy_plan *p);
 
+/* One FP64 solve (device pointers, as chy_solve with CHY_PTR_DEVICE and no
+ * diag) that allocates nothing: no device allocation, no free, no allocating
+ * library routine during the call.  It has no reference counterpart.  It is
+ * for callers whose device memory is fully committed once the plan exists,
+ * for example a simulation that reserves the rest of the GPU for its own
+ * arrays, or a time-step loop that must not call the allocator.
+ * Its per-solve work space is one static 8 MiB device array per device:
+ * enough for the FP64 work space of a 64 x 32 x 64 grid (3.5 MiB, the
+ * reference's CPU-run size) or 64 x 32 x 128 (6.5 MiB).  Grids that need more
+ * return CHY_ERR_CAPACITY (chy_last_error gives the size); mixed plans return
+ * CHY_ERR_UNSUPPORTED.  The array is cleared (cudaMemsetAsync) at the
+ * start of every call.  The first call on each device looks the array up
+ * (cudaGetSymbolAddress) with that device current; make it before any
+ * stream capture starts.  All calls on one device share the array, so calls
+ * that overlap in time (several streams or threads) race: serialise them.
+ * Asynchronous on `stream` like chy_solve. */
+int chy_solve_static(chy_plan *p, const double *rho, double *phi, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
