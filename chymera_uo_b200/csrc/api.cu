@@ -105,6 +105,7 @@ void chy_plan_destroy(chy_plan *p)
     cudaFree(p->d_tables);
     cudaFree(p->d_work);
     cudaFree(p->stage);
+    cudaFree(p->coef_dev);
     for (int i = 0; i < chy_plan::kStageSlots; i++) {
         if (p->ev_in[i]) cudaEventDestroy(p->ev_in[i]);
         if (p->ev_done[i]) cudaEventDestroy(p->ev_done[i]);
@@ -251,6 +252,30 @@ int chy_plan_set_coef(chy_plan *p, double *coef_dev)
 {
     if (!p) return fail(CHY_ERR_ARG, "null plan");
     p->w.coef = coef_dev;
+    p->coef_host = nullptr;
+    return CHY_OK;
+}
+
+int chy_plan_set_coef_host(chy_plan *p, double *coef_host)
+{
+    if (!p) return fail(CHY_ERR_ARG, "null plan");
+    if (!coef_host) {
+        p->coef_host = nullptr;
+        p->w.coef = nullptr;
+        return CHY_OK;
+    }
+    if (!p->coef_dev) {
+        const HostPlan &hp = p->hp;
+        const size_t n = (size_t)(hp.J + 2) * (hp.K + 2) * (hp.L / 2) * 2;
+        if (cudaMalloc(&p->coef_dev, n * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            p->coef_dev = nullptr;
+            return fail(CHY_ERR_NOMEM, "COEF device buffer");
+        }
+        p->coef_bytes = n * sizeof(double);
+    }
+    p->coef_host = coef_host;
+    p->w.coef = p->coef_dev;
     return CHY_OK;
 }
 
@@ -264,7 +289,7 @@ int chy_plan_set_refine(chy_plan *p, int corrections)
 long long chy_plan_device_bytes(const chy_plan *p)
 {
     if (!p) return 0;
-    return (long long)(p->table_bytes + p->work_bytes + p->stage_bytes);
+    return (long long)(p->table_bytes + p->work_bytes + p->stage_bytes + p->coef_bytes);
 }
 
 long long chy_plan_bytes_per_solve(const chy_plan *p)
@@ -431,7 +456,8 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
     // s_h2d, solve on the caller's stream, copy out on s_d2h.  A slot is
     // reused only after its previous copy out has finished.
     const size_t vb = p->nvol * sizeof(double), plane = J2 * K2 * sizeof(double);
-    const int c = p->stage_chunk, R = chy_plan::kStageSlots;
+    // with a host COEF destination, one solve per chunk (COEF is per solve)
+    const int c = p->coef_host ? 1 : p->stage_chunk, R = chy_plan::kStageSlots;
     bool used[chy_plan::kStageSlots] = {};
     CHY_CUDA(cudaEventRecord(p->ev_start, s));
     CHY_CUDA(cudaStreamWaitEvent(p->s_h2d, p->ev_start, 0));
@@ -456,8 +482,14 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         }
         CHY_CUDA(cudaEventRecord(p->ev_in[slot], p->s_h2d));
         CHY_CUDA(cudaStreamWaitEvent(s, p->ev_in[slot], 0));
+        // COEF cells the solve leaves alone (X1 = 0, pot/pot3.f:106) keep the
+        // caller's values: the device buffer starts from the host array
+        if (p->coef_host)
+            CHY_CUDA(cudaMemcpyAsync(p->coef_dev, p->coef_host, p->coef_bytes, cudaMemcpyHostToDevice, s));
         st = run_batch(p, bp, nb, s);
         if (st != CHY_OK) return st;
+        if (p->coef_host)
+            CHY_CUDA(cudaMemcpyAsync(p->coef_host, p->coef_dev, p->coef_bytes, cudaMemcpyDeviceToHost, s));
         if (diag) {
             // diagnostics are read per chunk: this synchronises the pipeline
             st = fetch_diag(p, diag, nb, first, s);

@@ -38,6 +38,9 @@ struct chy_plan {
     cudaEvent_t ev_start = nullptr;
     cudaEvent_t ev_in[kStageSlots] = {}, ev_done[kStageSlots] = {}, ev_out[kStageSlots] = {};
     double *h_diag = nullptr;   // pinned
+    double *coef_host = nullptr;   // /COEFS/ host destination (chy_plan_set_coef_host)
+    double *coef_dev = nullptr;    // device COEF buffer owned by the plan
+    size_t coef_bytes = 0;
     bool profile = false;
     // One event set per profiled launch sequence, read back lazily (after
     // the caller has synchronised) so profiling adds no host waits.

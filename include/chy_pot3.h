@@ -108,6 +108,12 @@ int chy_solve_batch(chy_plan *p, int n, const double *const *rho, double *const 
  * also write COEF(JMAX+2, KMAX+2, LMAX/2, 2) (amplitude, phase in degrees)
  * at coef_dev (device pointer, or NULL to stop). */
 int chy_plan_set_coef(chy_plan *p, double *coef_dev);
+/* The same for host-pointer solves into a host array (COEF as in /COEFS/):
+ * the plan allocates a device copy once, here, and each host-pointer solve
+ * copies it in before and out after the solve, so cells the reference leaves
+ * alone keep their values.  Host-pointer batches then run one solve per
+ * chunk.  NULL stops the output. */
+int chy_plan_set_coef_host(chy_plan *p, double *coef_host);
 
 /* Fixed number of refinement corrections for CHY_PREC_MIXED (default 1). */
 int chy_plan_set_refine(chy_plan *p, int corrections);
