@@ -105,6 +105,12 @@ def lib():
         L.chy_dbg_work.restype = ll
         L.chy_dbg_umma.argtypes = [vp, i, vp, vp, i]
         L.chy_dbg_umma.restype = i
+        L.chy_solve_multi.argtypes = [i, dpp, dpp, dpp, vp]
+        L.chy_solve_multi.restype = i
+        L.chy_solve_static.argtypes = [vp, vp, vp, vp]
+        L.chy_solve_static.restype = i
+        L.chy_plan_set_coef_host.argtypes = [vp, vp]
+        L.chy_plan_set_coef_host.restype = i
         _lib = L
     return _lib
 
@@ -248,6 +254,27 @@ class Plan:
     @staticmethod
     def _ptr(a, dev):
         return a.data_ptr() if dev else a.ctypes.data
+
+
+def solve_multi(plans, rhos, phis=None, stream=None):
+    """Densities of several grids in one stream-ordered call (chy_solve_multi):
+    rhos[i] (CUDA tensor, Fortran layout) is solved with plans[i]; returns the
+    PHI tensors (new ones unless phis is given)."""
+    import torch
+    n = len(rhos)
+    if len(plans) != n:
+        raise ValueError("one plan per density")
+    if phis is None:
+        phis = [fortran_zeros_cuda(p.shape, device=r.device) for p, r in zip(plans, rhos)]
+    for p, r, f in zip(plans, rhos, phis):
+        p._validate(r, True)
+        p._validate(f, True)
+    pp = (C.c_void_p * n)(*[p._p.value for p in plans])
+    rp = (C.c_void_p * n)(*[r.data_ptr() for r in rhos])
+    fp = (C.c_void_p * n)(*[f.data_ptr() for f in phis])
+    s = torch.cuda.current_stream() if stream is None else stream
+    _check(lib().chy_solve_multi(n, pp, rp, fp, C.c_void_p(s.cuda_stream)))
+    return phis
 
 
 def fortran_zeros_cuda(shape, device="cuda"):

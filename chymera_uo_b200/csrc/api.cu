@@ -1,8 +1,10 @@
 // api.cu -- the C ABI of libchy_pot3 (include/chy_pot3.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -508,6 +510,97 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
     return CHY_OK;
 }
 
+// ---------------------------------------------------------------------------
+// chy_solve_multi: densities of several grids in one stream-ordered call
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kMultiStreams = 8;
+struct StreamPool {
+    cudaStream_t streams[kMultiStreams] = {};
+    cudaEvent_t join[kMultiStreams] = {};
+    cudaEvent_t fork = nullptr;
+    bool ready = false;
+};
+std::mutex g_pool_mu;
+StreamPool g_pools[64];
+
+// Per-device side streams and fork/join events, created on first use.
+int stream_pool(StreamPool **out)
+{
+    int dev = 0;
+    CHY_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(CHY_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    StreamPool &sp = g_pools[dev];
+    if (!sp.ready) {
+        CHY_CUDA(cudaEventCreateWithFlags(&sp.fork, cudaEventDisableTiming));
+        for (int i = 0; i < kMultiStreams; i++) {
+            CHY_CUDA(cudaStreamCreateWithFlags(&sp.streams[i], cudaStreamNonBlocking));
+            CHY_CUDA(cudaEventCreateWithFlags(&sp.join[i], cudaEventDisableTiming));
+        }
+        sp.ready = true;
+    }
+    *out = &sp;
+    return CHY_OK;
+}
+}  // namespace
+
+extern "C" int chy_solve_multi(int n, chy_plan *const *plans, const double *const *rho, double *const *phi,
+                               void *stream)
+{
+    if (n < 0 || (n > 0 && (!plans || !rho || !phi))) return fail(CHY_ERR_ARG, "null arrays");
+    if (n == 0) return CHY_OK;
+    // group the requests by plan, largest total volume first
+    std::vector<chy_plan *> order;
+    std::vector<std::vector<int>> members;
+    for (int i = 0; i < n; i++) {
+        if (!plans[i] || !rho[i] || !phi[i]) return fail(CHY_ERR_ARG, "null plan or buffer in request list");
+        size_t g = 0;
+        while (g < order.size() && order[g] != plans[i]) g++;
+        if (g == order.size()) {
+            order.push_back(plans[i]);
+            members.emplace_back();
+        }
+        members[g].push_back(i);
+    }
+    std::vector<size_t> rank(order.size());
+    for (size_t g = 0; g < rank.size(); g++) rank[g] = g;
+    std::sort(rank.begin(), rank.end(), [&](size_t a, size_t b) {
+        return order[a]->nvol * members[a].size() > order[b]->nvol * members[b].size();
+    });
+    cudaStream_t s = (cudaStream_t)stream;
+    StreamPool *sp = nullptr;
+    int st = stream_pool(&sp);
+    if (st != CHY_OK) return st;
+    const int S = (int)std::min(order.size(), (size_t)kMultiStreams);
+    CHY_CUDA(cudaEventRecord(sp->fork, s));
+    for (int i = 0; i < S; i++) CHY_CUDA(cudaStreamWaitEvent(sp->streams[i], sp->fork, 0));
+    for (size_t r = 0; r < rank.size(); r++) {
+        const size_t g = rank[r];
+        chy_plan *p = order[g];
+        const std::vector<int> &idx = members[g];
+        cudaStream_t gs = sp->streams[r % S];
+        for (size_t first = 0; first < idx.size();) {
+            const int nb = (int)std::min(idx.size() - first, (size_t)std::min(p->max_batch, kMaxBatchPtrs));
+            BatchPtrs bp{};
+            for (int i = 0; i < nb; i++) {
+                bp.rho[i] = rho[idx[first + i]];
+                bp.phi[i] = phi[idx[first + i]];
+            }
+            st = run_batch(p, bp, nb, gs);
+            if (st != CHY_OK) return st;
+            first += nb;
+        }
+    }
+    for (int i = 0; i < S; i++) {
+        CHY_CUDA(cudaEventRecord(sp->join[i], sp->streams[i]));
+        CHY_CUDA(cudaStreamWaitEvent(s, sp->join[i], 0));
+    }
+    return CHY_OK;
+}
+
+int chy_internal_run_batch(chy_plan *p, const BatchPtrs &bp, int nb, cudaStream_t s) { return run_batch(p, bp, nb, s); }
+
 extern "C" int chy_solve(chy_plan *p, const double *rho, double *phi, chy_diag *diag, int ptr_kind,
                          void *stream)
 {
@@ -537,7 +630,6 @@ extern "C" long long chy_dbg_work(chy_plan *p, const char *name, double *out, lo
     return (long long)cnt;
 }
 
-#include <mutex>
 #include <unordered_map>
 
 cudaError_t chy::ensure_smem(const void *kernel, size_t bytes)

@@ -52,6 +52,9 @@ struct chy_plan {
     MixedState *mx = nullptr;
 };
 
+// One launch sequence over nb device-pointer solves (api.cu).
+int chy_internal_run_batch(chy_plan *p, const chy::BatchPtrs &bp, int nb, cudaStream_t s);
+
 // Mixed-precision mode solve (k_mixed.cu).
 bool chy_mixed_supported(const chy::HostPlan *hp);
 // Appends the mixed path's tables to the packed table image; returns offset.

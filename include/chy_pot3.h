@@ -104,6 +104,16 @@ int chy_solve(chy_plan *p, const double *rho, double *phi, chy_diag *diag, int p
 int chy_solve_batch(chy_plan *p, int n, const double *const *rho, double *const *phi,
                     chy_diag *diag, int ptr_kind, void *stream);
 
+/* n densities of possibly different grids (device pointers): request i is
+ * solved with plans[i].  Requests that share a plan are batched (up to its
+ * max_batch per launch sequence); different plans run concurrently on side
+ * streams forked from `stream` and joined back into it, so the call is
+ * ordered on `stream` like chy_solve_batch and makes no host wait.  The first
+ * call on a device creates the side streams.  A plan may appear in only one
+ * call at a time; calls from several host threads must be serialised.  No
+ * reference counterpart (the reference solves one grid per run). */
+int chy_solve_multi(int n, chy_plan *const *plans, const double *const *rho, double *const *phi, void *stream);
+
 /* Optional /COEFS/ output (pot/pot3.f:105-132): when set, the next solves
  * also write COEF(JMAX+2, KMAX+2, LMAX/2, 2) (amplitude, phase in degrees)
  * at coef_dev (device pointer, or NULL to stop). */
