@@ -51,6 +51,16 @@ class ChyDiag(C.Structure):
                 "corr_rel": list(self.corr_rel[: max(0, self.iterations)])}
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget", C.c_longlong), ("precision", C.c_int), ("max_batch", C.c_int),
+                ("arena_fraction", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_longlong), ("batches", C.c_longlong), ("size_classes", C.c_int),
+                ("plan_bytes", C.c_longlong), ("arena_bytes", C.c_longlong)]
+
+
 class ChyError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"chy status {status}: {msg}")
@@ -111,6 +121,15 @@ def lib():
         L.chy_solve_static.restype = i
         L.chy_plan_set_coef_host.argtypes = [vp, vp]
         L.chy_plan_set_coef_host.restype = i
+        L.chy_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(vp)]
+        L.chy_server_create.restype = i
+        L.chy_server_submit.argtypes = [vp, C.POINTER(ChyGrid), vp, vp, C.POINTER(ll)]
+        L.chy_server_submit.restype = i
+        L.chy_server_wait.argtypes = [vp, ll, C.POINTER(C.c_double)]
+        L.chy_server_wait.restype = i
+        L.chy_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+        L.chy_server_get_stats.restype = i
+        L.chy_server_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -254,6 +273,61 @@ class Plan:
     @staticmethod
     def _ptr(a, dev):
         return a.data_ptr() if dev else a.ctypes.data
+
+
+class Server:
+    """Continuous-batching request loop (chy_server_*): submit host arrays
+    (numpy, Fortran order; pinned memory gives full copy bandwidth) from any
+    thread, wait for each ticket."""
+
+    def __init__(self, precision: str = "mixed", hbm_budget: int = 0, max_batch: int = 8,
+                 arena_fraction: float = 0.5):
+        o = ServerOpts(hbm_budget, CHY_PREC_MIXED if precision == "mixed" else CHY_PREC_FP64, max_batch,
+                       arena_fraction)
+        p = C.c_void_p()
+        _check(lib().chy_server_create(C.byref(o), C.byref(p)))
+        self._p = p
+        self._keep = {}
+
+    def submit(self, g: ChyGrid, rho: np.ndarray, phi: np.ndarray) -> int:
+        shape = (g.jmax + 2, g.kmax + 2, g.lmax)
+        for a in (rho, phi):
+            if a.shape != shape or a.dtype != np.float64 or not a.flags.f_contiguous:
+                raise ValueError(f"expected Fortran-ordered float64 array of shape {shape}")
+        t = C.c_longlong(0)
+        _check(lib().chy_server_submit(self._p, C.byref(g), rho.ctypes.data, phi.ctypes.data, C.byref(t)))
+        self._keep[t.value] = (g, rho, phi)
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        """Blocks until the request is done; returns its latency in ms."""
+        ms = C.c_double(0.0)
+        st = lib().chy_server_wait(self._p, ticket, C.byref(ms))
+        self._keep.pop(ticket, None)
+        _check(st)
+        return ms.value
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().chy_server_get_stats(self._p, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if self._p:
+            lib().chy_server_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pinned_fortran(shape):
+    """A pinned host numpy array of the given Fortran shape (float64)."""
+    import torch
+    return torch.empty(tuple(shape[::-1]), dtype=torch.float64, pin_memory=True).numpy().transpose()
 
 
 def solve_multi(plans, rhos, phis=None, stream=None):

@@ -283,7 +283,11 @@ int chy_plan_set_coef_host(chy_plan *p, double *coef_host)
 
 int chy_plan_set_refine(chy_plan *p, int corrections)
 {
-    if (!p || corrections < 0 || corrections > 8) return fail(CHY_ERR_ARG, "corrections must be 0..8");
+    if (!p || corrections < 0 || corrections > 7) return fail(CHY_ERR_ARG, "corrections must be 0..7");
+    if (corrections >= 2) {
+        const int st = chy_mixed_ensure_iterate(p);
+        if (st != CHY_OK) return fail(st, "FP64 iterate for two or more corrections");
+    }
     p->refine = corrections;
     return CHY_OK;
 }
@@ -291,7 +295,7 @@ int chy_plan_set_refine(chy_plan *p, int corrections)
 long long chy_plan_device_bytes(const chy_plan *p)
 {
     if (!p) return 0;
-    return (long long)(p->table_bytes + p->work_bytes + p->stage_bytes + p->coef_bytes);
+    return (long long)(p->table_bytes + p->work_bytes + p->stage_bytes + p->coef_bytes + chy_mixed_iterate_bytes(p));
 }
 
 long long chy_plan_bytes_per_solve(const chy_plan *p)

@@ -81,6 +81,7 @@ struct MixedState {
     size_t o_aimg = 0, o_lam = 0;   // offsets into the packed table image
     MixedDev dev{};
     double *h_corr = nullptr;       // pinned [max_batch][L][8][2]
+    size_t xbuf_bytes = 0;          // FP64 iterate (two or more corrections)
     int *h_err = nullptr;           // pinned
 };
 
@@ -985,12 +986,14 @@ void chy_mixed_bind_tables(chy_plan *p, char *dev_base)
     p->mx->dev.lam = reinterpret_cast<const float *>(p->d_tables + lam_off);
 }
 
+// Per-mode correction sums and the error word; the FP64 iterate of the
+// general path (two or more corrections) is allocated by
+// chy_mixed_ensure_iterate when such a count is set.
 size_t chy_mixed_work_doubles(const chy_plan *p)
 {
     if (p->precision != CHY_PREC_MIXED) return 0;
     const chy::HostPlan &hp = p->hp;
-    const size_t per = (size_t)hp.L * hp.K * hp.J + (size_t)hp.L * 16;
-    return per * p->max_batch + 8;
+    return (size_t)hp.L * 16 * p->max_batch + 8;
 }
 
 void chy_mixed_bind_work(chy_plan *p, double *base)
@@ -1000,8 +1003,8 @@ void chy_mixed_bind_work(chy_plan *p, double *base)
     const chy::HostPlan &hp = p->hp;
     d.sxb = (size_t)hp.L * hp.K * hp.J;
     d.scorr = (size_t)hp.L * 16;
-    d.xbuf = base;
-    d.corr = base + d.sxb * p->max_batch;
+    d.xbuf = nullptr;
+    d.corr = base;
     d.err = reinterpret_cast<int *>(d.corr + d.scorr * p->max_batch);
     d.ntile = round64(hp.J);
     if (p->precision == CHY_PREC_MIXED) {
@@ -1016,6 +1019,7 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
     MixedDev d = p->mx->dev;
     d.nit = 1 + p->refine;
     if (d.nit > 8) d.nit = 8;
+    if (d.nit > 2 && !d.xbuf) return CHY_ERR_NOT_SETUP;
     // the kernel streams X and the iterate with 16-byte async copies
     if ((reinterpret_cast<uintptr_t>(p->w.X) | reinterpret_cast<uintptr_t>(d.xbuf)) % 16 != 0 || p->hp.J % 16 != 0)
         return CHY_ERR_ARG;
@@ -1066,9 +1070,27 @@ void chy_mixed_fill_diag(const chy_plan *p, int slot, chy_diag *d)
     }
 }
 
+size_t chy_mixed_iterate_bytes(const chy_plan *p) { return p->mx ? p->mx->xbuf_bytes : 0; }
+
+int chy_mixed_ensure_iterate(chy_plan *p)
+{
+    if (p->precision != CHY_PREC_MIXED || !p->mx || p->mx->dev.xbuf) return CHY_OK;
+    MixedDev &d = p->mx->dev;
+    const size_t bytes = d.sxb * p->max_batch * sizeof(double);
+    if (cudaMalloc(&d.xbuf, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        d.xbuf = nullptr;
+        return CHY_ERR_NOMEM;
+    }
+    p->mx->xbuf_bytes = bytes;
+    // columns >= M and rows >= NZ are read as zeros and never written
+    return cudaMemset(d.xbuf, 0, bytes) == cudaSuccess ? CHY_OK : CHY_ERR_CUDA;
+}
+
 void chy_mixed_release(chy_plan *p)
 {
     if (!p->mx) return;
+    cudaFree(p->mx->dev.xbuf);
     cudaFreeHost(p->mx->h_corr);
     cudaFreeHost(p->mx->h_err);
     delete p->mx;

@@ -69,4 +69,7 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches);
 // correction norms; CHY_ERR_TIMEOUT if a bounded wait expired.
 int chy_mixed_collect(chy_plan *p, int nb);
 void chy_mixed_fill_diag(const chy_plan *p, int slot, chy_diag *d);
+// Allocates the FP64 iterate used when two or more corrections are set.
+int chy_mixed_ensure_iterate(chy_plan *p);
+size_t chy_mixed_iterate_bytes(const chy_plan *p);
 void chy_mixed_release(chy_plan *p);

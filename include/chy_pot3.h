@@ -114,6 +114,40 @@ int chy_solve_batch(chy_plan *p, int n, const double *const *rho, double *const 
  * reference counterpart (the reference solves one grid per run). */
 int chy_solve_multi(int n, chy_plan *const *plans, const double *const *rho, double *const *phi, void *stream);
 
+/* ---- serving: continuous batching of solve requests ----------------------
+ * No reference counterpart.  A server keeps one size class per distinct grid
+ * (resident plans: tables + work space, two lanes so that the copies of one
+ * batch overlap the solves of the previous one) and a dispatcher thread.
+ * Requests queue from any thread; a request is admitted into its class's next
+ * batch as soon as device buffers for it fit in the server's arena, so
+ * requests that arrive while others run join the next batch of their grid;
+ * classes run concurrently on their own streams.  Results do not depend on
+ * batching (every reduction has a fixed per-solve order). */
+typedef struct chy_server chy_server;
+typedef struct chy_server_opts {
+    long long hbm_budget;      /* device bytes for plans + request buffers; 0: 3/4 of free */
+    int precision;             /* CHY_PREC_MIXED (grids it does not cover use FP64) or _FP64 */
+    int max_batch;             /* solves per launch sequence (default 8, <= 64)            */
+    double arena_fraction;     /* share of the budget for request buffers (default 0.5)    */
+} chy_server_opts;
+typedef struct chy_server_stats {
+    long long completed, batches;
+    int size_classes;
+    long long plan_bytes, arena_bytes;
+} chy_server_stats;
+/* Starts the dispatcher on the current device; allocates the arena. */
+int chy_server_create(const chy_server_opts *o, chy_server **out);
+/* Queues one solve of grid g (arrays copied now): rho is read and phi written
+ * (the reference's write set) asynchronously; both must stay valid until
+ * chy_server_wait returns.  Pinned host memory gives full copy bandwidth. */
+int chy_server_submit(chy_server *s, const chy_grid *g, const double *rho, double *phi, long long *ticket);
+/* Blocks until the request is done; returns its status and the latency from
+ * submission to completion (host clock, ms). */
+int chy_server_wait(chy_server *s, long long ticket, double *latency_ms);
+int chy_server_get_stats(chy_server *s, chy_server_stats *out);
+/* Finishes the queued requests, then releases everything. */
+void chy_server_destroy(chy_server *s);
+
 /* Optional /COEFS/ output (pot/pot3.f:105-132): when set, the next solves
  * also write COEF(JMAX+2, KMAX+2, LMAX/2, 2) (amplitude, phase in degrees)
  * at coef_dev (device pointer, or NULL to stop). */
@@ -125,7 +159,10 @@ int chy_plan_set_coef(chy_plan *p, double *coef_dev);
  * chunk.  NULL stops the output. */
 int chy_plan_set_coef_host(chy_plan *p, double *coef_host);
 
-/* Fixed number of refinement corrections for CHY_PREC_MIXED (default 1). */
+/* Fixed number of refinement corrections for CHY_PREC_MIXED, 0..7 (default
+ * 1).  Up to one correction the first solution stays in tensor memory; two or
+ * more keep an FP64 iterate in device memory, allocated by this call (one
+ * more grid volume per batch slot). */
 int chy_plan_set_refine(chy_plan *p, int corrections);
 
 /* Bytes of device work space the plan holds (tables + per-solve scratch). */

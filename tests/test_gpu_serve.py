@@ -1,0 +1,69 @@
+"""The serving loop (chy_server_*): requests of mixed grid sizes arrive on a
+Poisson clock while earlier ones are on the GPU; each result must equal the
+same density solved alone through a plain plan (bitwise: the kernels reduce in
+a fixed order per solve), mixed-precision results stay within rel. L2 1e-10
+of the FP64 path, and requests of one grid share batches."""
+import threading
+
+import numpy as np
+import pytest
+
+from chymera_uo_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(64, 32, 64), (128, 64, 128), (64, 32, 128), (256, 128, 256), (128, 32, 64)]
+
+
+def _requests(n, seed=7):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        J, K, L = SIZES[int(rng.integers(len(SIZES)))] if i >= 8 else SIZES[0]
+        rho = synth.disk_density(J, K, L, 10**6 + i, slope=float(rng.uniform(-2, -1)),
+                                 h=float(rng.uniform(0.03, 0.1)), spiral=True, spectrum=True)
+        out.append(((J, K, L), rho))
+    return out
+
+
+def test_served_results_equal_solves_alone(chylib):
+    reqs = _requests(24)
+    srv = chylib.Server("mixed", hbm_budget=24 << 30, max_batch=4)
+    phis = []
+    for (J, K, L), rho in reqs:
+        a = chylib.pinned_fortran(rho.shape)
+        a[...] = rho
+        f = chylib.pinned_fortran(rho.shape)
+        f[...] = 3.0
+        phis.append((a, f))
+    tickets = [None] * len(reqs)
+    rng = np.random.default_rng(1)
+
+    def producer():
+        import time
+        for i, ((J, K, L), _) in enumerate(reqs):
+            if i >= 8:    # the first eight arrive at once (one grid), the rest on a Poisson clock
+                time.sleep(float(rng.exponential(0.002)))
+            tickets[i] = srv.submit(chylib.grid(J, K, L), *phis[i])
+
+    th = threading.Thread(target=producer)
+    th.start()
+    th.join()
+    lat = [srv.wait(t) for t in tickets]
+    stats = srv.stats()
+    srv.close()
+    assert stats["completed"] == len(reqs) and stats["batches"] < len(reqs)
+    assert all(x > 0 for x in lat)
+
+    plans, plans64 = {}, {}
+    for ((J, K, L), rho), (_, f) in zip(reqs, phis):
+        key = (J, K, L)
+        if key not in plans:
+            plans[key] = chylib.Plan(chylib.grid(J, K, L), "mixed", 1)
+            plans64[key] = chylib.Plan(chylib.grid(J, K, L), "fp64", 1)
+        alone = plans[key].solve(rho, np.full_like(rho, 3.0, order="F"))
+        assert np.array_equal(alone, f), key
+        ref = plans64[key].solve(rho)
+        ws = (slice(0, J + 1), slice(0, K + 1))
+        assert np.linalg.norm((f[ws] - ref[ws]).ravel()) <= 1e-10 * np.linalg.norm(ref[ws].ravel())
+        assert np.all(f[:, K + 1, :] == 3.0)
