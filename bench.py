@@ -200,6 +200,156 @@ def cpu_baseline(rhos, budget_s, max_solves):
     return rec, outs
 
 
+# ---------------------------------------------------------------- batched workload
+def run_batch_workload(args):
+    """64 seeded disks of uneven sizes (JMAX in {64,128,256}, KMAX in
+    {32,64,128}, LMAX in {64,128,256}, random slope and H/r): one step = one
+    replay of a CUDA graph holding chy_solve_multi over all of them; the FP64
+    path is timed the same way.  Single GPU (replicas as for pot3)."""
+    import torch
+    import chymera_uo_b200 as chy
+    from chymera_uo_b200 import synth
+    rank, local, ws = dist_info()
+    torch.cuda.set_device(local)
+    n = 64
+    dens = [synth.config_density(4, i) for i in range(n)]
+    rhos = [chy.to_cuda_fortran(r) for r, _ in dens]
+    res = {}
+    for prec in ("mixed", "fp64"):
+        cache = {}
+        plans = []
+        for _, g in dens:
+            key = (g.jmax, g.kmax, g.lmax)
+            if key not in cache:
+                cache[key] = chy.Plan(chy.grid(*key), prec, 8)
+            plans.append(cache[key])
+        outs = [chy.fortran_zeros_cuda(p.shape) for p in plans]
+        chy.solve_multi(plans, rhos, outs)          # side streams and smem attributes before capture
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            chy.solve_multi(plans, rhos, outs)
+        for _ in range(args.warmup):
+            graph.replay()
+        torch.cuda.synchronize()
+        launches0 = sum(p.launches for p in cache.values())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record()
+            for _ in range(args.steps):
+                graph.replay()
+            e1.record()
+            torch.cuda.synchronize()
+        res[prec] = {"ms": e0.elapsed_time(e1), "outs": outs, "clocks": clk.summary(),
+                     "sizes": len(cache), "plans": cache}
+        del graph
+    worst = 0.0
+    for (_, g), a, b in zip(dens, res["mixed"]["outs"], res["fp64"]["outs"]):
+        sl = (slice(0, g.jmax + 1), slice(0, g.kmax + 1))
+        worst = max(worst, float(torch.linalg.vector_norm(a[sl] - b[sl]) / torch.linalg.vector_norm(b[sl])))
+    ms = res["mixed"]["ms"]
+    value = n * args.steps / (ms * 1e-3)
+    line = {"metric": "pot3 solves/s, 64 uneven grids per CUDA-graph replay (mixed vs FP64)", "value": value,
+            "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed: f16 hi/lo tensor-core + f32 + f64", "data": "synthetic",
+            "config": {"workload": "batched: 64 seeded disks, JMAX {64,128,256} x KMAX {32,64,128} x "
+                                   "LMAX {64,128,256}, slope U[-2,-1], H/r U[0.03,0.1]",
+                       "distinct_grids": res["mixed"]["sizes"], "solves_per_step": n,
+                       "launch": "one CUDA graph replay of chy_solve_multi per step",
+                       "l2": "inputs larger than L2 (all 64 densities resident)"},
+            "fp64_gpu": {"value": n * args.steps / (res["fp64"]["ms"] * 1e-3), "unit": UNIT,
+                         "ms_per_step": res["fp64"]["ms"] / args.steps},
+            "accuracy": {"rel_l2_mixed_vs_fp64_max": worst},
+            "clocks": res["mixed"]["clocks"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- serving workload
+def run_serving_workload(args):
+    """Poisson request streams (mean rates --rates) of seeded disks with the
+    serving mix of grid sizes (20% 512x128x512, the rest drawn from the batched
+    size set) through chy_server; reports solves/s and p50/p99 latency per rate
+    for the mixed-precision server and the plain FP64 server."""
+    import threading
+    import torch
+    import chymera_uo_b200 as chy
+    from chymera_uo_b200 import synth
+    rank, local, ws = dist_info()
+    torch.cuda.set_device(local)
+    # a pool of distinct requests, reused round robin (a pool entry is
+    # resubmitted only after its previous request finished)
+    pool_n = 48
+    pool = []
+    for i in range(pool_n):
+        rho, g = synth.config_density(5, i)
+        a = chy.pinned_fortran(rho.shape)
+        a[...] = rho
+        f = chy.pinned_fortran(rho.shape)
+        f[...] = 0.0
+        pool.append(((g.jmax, g.kmax, g.lmax), a, f))
+    rates = [float(r) for r in args.rates.split(",") if r]
+    out = []
+    for prec in ("mixed", "fp64"):
+        srv = chy.Server(prec, hbm_budget=96 << 30, max_batch=4)
+        grids = {k: chy.grid(*k) for k, _, _ in pool}
+        # warm every size class once (plans are created on first use)
+        for t in [srv.submit(grids[k], a, f) for k, a, f in pool]:
+            srv.wait(t)
+        for rate in rates:
+            n = args.requests
+            rng = np.random.default_rng(int(rate))
+            gaps = rng.exponential(1.0 / rate, n)
+            tickets = [None] * n
+            last = [None] * pool_n
+            lat = [0.0] * n
+            lock = threading.Lock()
+
+            def producer():
+                t0 = time.perf_counter()
+                due = t0
+                for i in range(n):
+                    due += gaps[i]
+                    d = due - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    j = i % pool_n
+                    if last[j] is not None:
+                        lat[last[j]] = srv.wait(tickets[last[j]])
+                    k, a, f = pool[j]
+                    with lock:
+                        tickets[i] = srv.submit(grids[k], a, f)
+                    last[j] = i
+
+            st0 = srv.stats()
+            t_start = time.perf_counter()
+            th = threading.Thread(target=producer)
+            th.start()
+            th.join()
+            for j in range(pool_n):
+                if last[j] is not None:
+                    lat[last[j]] = srv.wait(tickets[last[j]])
+            wall = time.perf_counter() - t_start
+            st1 = srv.stats()
+            out.append({"precision": prec, "rate_req_s": rate, "requests": n, "solves_per_s": n / wall,
+                        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "batches": st1["batches"] - st0["batches"]})
+        srv.close()
+    line = {"metric": "pot3 serving: solves/s and p50/p99 latency vs Poisson arrival rate (mixed vs FP64)",
+            "value": max(r["solves_per_s"] for r in out if r["precision"] == "mixed"), "unit": UNIT,
+            "n_gpus": ws, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "serving: seeded disks, 20% 512x128x512, 80% from the batched size set; "
+                                   f"{pool_n} distinct requests reused round robin; pinned host buffers; "
+                                   "latency = submit to completion on the host clock",
+                       "server": "chy_server, max_batch 4, two lanes per grid"},
+            "per_rate": out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- GPU arm
 def rel_l2(a, b):
     return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
@@ -216,11 +366,20 @@ def main():
     ap.add_argument("--latency-samples", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="pot3", choices=["pot3", "batch", "serving"],
+                    help="pot3: 256x128x256 mixed (default); batch: 64 uneven grids from one captured "
+                         "graph; serving: Poisson request stream with p50/p99 latency")
+    ap.add_argument("--rates", default="200,1000,5000", help="serving: mean arrival rates (req/s)")
+    ap.add_argument("--requests", type=int, default=400, help="serving: requests per rate")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch_workload(args)
+    if args.workload == "serving":
+        return run_serving_workload(args)
 
     import torch
     import chymera_uo_b200 as chy
