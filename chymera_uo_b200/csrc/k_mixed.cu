@@ -236,6 +236,18 @@ __device__ __forceinline__ void tm_ld1_nw(uint32_t taddr, float &v)
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=f"(v) : "r"(taddr) : "memory");
 }
 
+__device__ __forceinline__ void tm_wait_ld32(float *v, float *w)
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]),
+                   "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]),
+                   "+f"(v[15]), "+f"(w[0]), "+f"(w[1]), "+f"(w[2]), "+f"(w[3]), "+f"(w[4]), "+f"(w[5]), "+f"(w[6]),
+                   "+f"(w[7]), "+f"(w[8]), "+f"(w[9]), "+f"(w[10]), "+f"(w[11]), "+f"(w[12]), "+f"(w[13]),
+                   "+f"(w[14]), "+f"(w[15])
+                 :
+                 : "memory");
+}
+
 __device__ __forceinline__ void tm_wait_ld18(float *v, float &a, float &b)
 {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
@@ -451,7 +463,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             const bool last = it == nit - 1;
             const bool res_x = kRes && it > 0;          // x0 read from tensor memory
             const uint32_t acc = res_x ? 256u : 0u;     // product / sweep columns
-            double sxx = 0.0;                           // kRes: sum of x0^2
+            float sxf = 0.f;                            // kRes: sum of x0^2 (unscaled)
             // ---- residual r = Y - A_m x (FP64) -> TMEM cols [256, 256+NT) as FP32.
             // Out-of-range neighbours read as 0; their stencil coefficients
             // (AN(1), CN(KMAX-1), AM(1), CM(JMAX-1)) are 0 too.  JMAX is a
@@ -488,10 +500,12 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     const int c0 = c * kRingC;
                     float xc[16], xlf = 0.f, xrt = 0.f;
                     if (res_x) {
+                        // the tensor-memory loads fly while the row copies land
                         const int jl = c0 + jb - 1, jr = c0 + jb + 16;
                         tm_ld16_nw(tmem + lane_base + c0 + jb, xc);
                         tm_ld1_nw(tmem + lane_base + (uint32_t)(jl < 0 ? 0 : jl), xlf);
                         tm_ld1_nw(tmem + lane_base + (uint32_t)(jr < NT ? jr : NT - 1), xrt);
+                        cp_async_wait<1>();
                         tm_wait_ld18(xc, xlf, xrt);
                         if (jl < 0) xlf = 0.f;
                         if (jr >= NT) xrt = 0.f;
@@ -504,30 +518,46 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
 #pragma unroll
                             for (int u = 0; u < 16; ++u) ed[16 + u] = xc[u];
                         }
+                    } else {
+                        cp_async_wait<1>();
                     }
-                    cp_async_wait<1>();
                     __syncthreads();
                     issue(c + 2);
-                    // branch-free: the folds are multiplied by zero where they do
-                    // not apply, cells outside the interior are selected away
+                    // right-hand side 4 pi G rho with the boundary folds
+                    // (pot/pot3.f:219-224): the row below the top boundary folds
+                    // row NZ (one thread), the column M fold lies in one chunk
                     const double *buf = ring + (c % 3) * kRingBuf;
                     const double *sy = buf + k * kRingS;
-                    double yv[16], yt[16];
+                    double yv[16];
 #pragma unroll
                     for (int u = 0; u < 16; u += 2) {
                         const double2 t2 = *reinterpret_cast<const double2 *>(sy + jb + u);
-                        const double2 t3 = *reinterpret_cast<const double2 *>(buf + NZ * kRingS + jb + u);
-                        yv[u] = t2.x;
-                        yv[u + 1] = t2.y;
-                        yt[u] = t3.x;
-                        yt[u + 1] = t3.y;
+                        yv[u] = t.pig4 * t2.x;
+                        yv[u + 1] = t.pig4 * t2.y;
                     }
-                    const double ytop = k == NZ - 1 ? t.cnmax : 0.0;
-                    const double yM = sy[max(min(M - c0, kRingC - 1), 0)];
+                    if (k == NZ - 1) {
+#pragma unroll
+                        for (int u = 0; u < 16; u += 2) {
+                            const double2 t3 = *reinterpret_cast<const double2 *>(buf + NZ * kRingS + jb + u);
+                            yv[u] = fma(-t.cnmax, t3.x, yv[u]);
+                            yv[u + 1] = fma(-t.cnmax, t3.y, yv[u + 1]);
+                        }
+                    }
+                    const int uM = M - 1 - (c0 + jb);   // uniform in the warp
+                    if (uM >= 0 && uM < 16) {
+                        const double yM = sy[M - c0];
+#pragma unroll
+                        for (int u = 0; u < 16; ++u)
+                            if (u == uM) yv[u] = fma(-t.cmmax, yM, yv[u]);
+                    }
                     float v[16];
                     if (res_x) {
-                        const float *eu = f_edge + ((c & 1) * 8 + warp - 1) * 32 + 16;   // row above lane 0
-                        const float *ed = f_edge + ((c & 1) * 8 + warp + 1) * 32;        // row below lane 31
+                        // rows above lane 0 and below lane 31 come from the
+                        // neighbouring warps' edges (all lanes load, two select)
+                        const float *eu = f_edge + ((c & 1) * 8 + (quad > 0 ? warp - 1 : warp)) * 32 + 16;
+                        const float *ed = f_edge + ((c & 1) * 8 + (quad < 3 ? warp + 1 : warp)) * 32;
+                        const bool top0 = lane == 0, bot31 = lane == 31;
+                        const float zu = quad > 0 ? 1.f : 0.f, zd = quad < 3 ? 1.f : 0.f;
                         double xd_[18];   // x0 at columns j-1 .. j+16 (unscaled)
                         xd_[0] = (double)xlf;
                         xd_[17] = (double)xrt;
@@ -538,20 +568,18 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                             const int j = c0 + jb + u;
                             float xu = __shfl_up_sync(0xffffffffu, xc[u], 1);
                             float xd = __shfl_down_sync(0xffffffffu, xc[u], 1);
-                            if (lane == 0) xu = quad > 0 ? eu[u] : 0.f;
-                            if (lane == 31) xd = quad < 3 ? ed[u] : 0.f;
+                            const float eu_u = eu[u] * zu, ed_u = ed[u] * zd;
+                            xu = top0 ? eu_u : xu;
+                            xd = bot31 ? ed_u : xd;
                             // A x0 / u0: u0 is a power of two, so scaling the sum is exact
                             double ax = (bnk + d_bm[j]) * xd_[u + 1];
                             ax = fma(an, (double)xu, ax);
                             ax = fma(cn, (double)xd, ax);
                             ax = fma(d_am[j], xd_[u], ax);
                             ax = fma(d_cm[j], xd_[u + 2], ax);
-                            double r = t.pig4 * yv[u];
-                            r = fma(-ytop, yt[u], r);
-                            r = fma(j == M - 1 ? -t.cmmax : 0.0, yM, r);
-                            r = fma(-u0, ax, r);
+                            const double r = fma(-u0, ax, yv[u]);
                             const bool in = krow && j < M;
-                            sxx = fma(in ? xd_[u + 1] : 0.0, xd_[u + 1], sxx);
+                            sxf = fmaf(in ? xc[u] : 0.f, xc[u], sxf);
                             v[u] = in ? (float)r : 0.f;
                             rmax = fmaxf(rmax, fabsf(v[u]));
                         }
@@ -559,10 +587,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
 #pragma unroll
                         for (int u = 0; u < 16; ++u) {
                             const int j = c0 + jb + u;
-                            double r = t.pig4 * yv[u];
-                            r = fma(-ytop, yt[u], r);
-                            r = fma(j == M - 1 ? -t.cmmax : 0.0, yM, r);
-                            v[u] = (krow && j < M) ? (float)r : 0.f;
+                            v[u] = (krow && j < M) ? (float)yv[u] : 0.f;
                             rmax = fmaxf(rmax, fabsf(v[u]));
                         }
                     }
@@ -834,33 +859,46 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     u0 = unscale;   // x0 stays in tensor memory columns [0, NT)
                     continue;
                 }
-                // X = x0 + delta (FP64), staged through sD[k][jj] to write rows
-                double *sD = reinterpret_cast<double *>(sBh);
+                // X = x0 + delta (FP64), staged through sD[buf][k][jj] to write
+                // rows; the next chunk's tensor-memory rows load while this
+                // chunk's rows are stored
                 double sd = 0.0, sx = 0.0;
                 const int jb = jh * 16;
+                float dv[16], xv[16];
+                tm_ld16_nw(tmem + lane_base + acc + jb, dv);
+                if (res_x) tm_ld16_nw(tmem + lane_base + jb, xv);
                 for (int c0 = 0; c0 < NT; c0 += 32) {
-                    float dv[16], xv[16];
-                    tm_ld16(tmem + lane_base + acc + c0 + jb, dv);
-                    if (res_x) tm_ld16(tmem + lane_base + c0 + jb, xv);
+                    double *sD = reinterpret_cast<double *>(sBh) + ((c0 >> 5) & 1) * (128 * 34);
+                    tm_wait_ld32(dv, xv);
 #pragma unroll
                     for (int u = 0; u < 16; ++u) {
                         const int j = c0 + jb + u;
                         const double dl = (double)dv[u] * unscale;
                         const double xn = (res_x ? (double)xv[u] * u0 : 0.0) + dl;
-                        sD[kq * 33 + jb + u] = xn;
+                        sD[kq * 34 + jb + u] = xn;
                         if (kq < NZ && j < M) {
                             sd += dl * dl;
                             sx += xn * xn;
                         }
                     }
                     __syncthreads();
-                    for (int i = tid; i < 128 * 32; i += 256) {
-                        const int k = i >> 5, jj = i & 31, j = c0 + jj;
-                        if (k < NZ && j < M) Xl[(size_t)k * J + j] = sD[k * 33 + jj];
+                    if (c0 + 32 < NT) {
+                        tm_ld16_nw(tmem + lane_base + acc + c0 + 32 + jb, dv);
+                        if (res_x) tm_ld16_nw(tmem + lane_base + c0 + 32 + jb, xv);
                     }
-                    __syncthreads();
+                    // rows of X in 16-byte pieces (J even: pieces never straddle
+                    // column M, which only the last piece of a row touches)
+                    for (int i = tid; i < 128 * 16; i += 256) {
+                        const int k = i >> 4, jj = 2 * (i & 15), j = c0 + jj;
+                        if (k >= NZ || j >= M) continue;
+                        const double2 val = *reinterpret_cast<const double2 *>(sD + k * 34 + jj);
+                        double *dst = Xl + (size_t)k * J + j;
+                        if (j + 1 < M) *reinterpret_cast<double2 *>(dst) = val;
+                        else *dst = val.x;
+                    }
                 }
-                block_sum3(sd, sx, sxx);
+                __syncthreads();
+                block_sum3(sd, sx, (double)sxf);
                 if (tid == 0) {
                     if (res_x) {   // the first solve's delta is x0 itself
                         cr[0] = d_red[16] * u0 * u0;
