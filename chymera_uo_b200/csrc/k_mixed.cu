@@ -302,6 +302,32 @@ __device__ __forceinline__ void put_split(uint8_t *hi, uint8_t *lo, int row, int
     *reinterpret_cast<__half *>(lo + o) = l;
 }
 
+// FP16 hi/lo split of 32 consecutive B-tile rows c0..c0+31 (K index kq, the
+// caller's TMEM lane), values already scaled.  Lane pairs (2i, 2i+1) swap
+// halves so that each thread writes the (k even, k odd) pair of one row as a
+// half2: rows c0+u for even lanes, c0+u+1 for odd lanes.  Same roundings as
+// put_split, element by element.
+__device__ __forceinline__ void split_rows32(uint8_t *hi, uint8_t *lo, const float *v, int c0, int kq, int lane,
+                                             int R)
+{
+    const int odd = lane & 1, ke = kq & ~1, kk = ke & 63, g = kk >> 3;
+    const uint32_t base = (uint32_t)((ke >> 6) * (R * 128) + ((kk & 7) << 1));
+#pragma unroll
+    for (int u = 0; u < 32; u += 2) {
+        const float send = odd ? v[u] : v[u + 1];
+        const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+        const float a = odd ? recv : v[u];        // K index ke
+        const float b = odd ? v[u + 1] : recv;    // K index ke + 1
+        const int row = c0 + u + odd;
+        const uint32_t off = base + (uint32_t)row * 128 + ((uint32_t)(g ^ (row & 7)) << 4);
+        const __half2 h = __floats2half2_rn(a, b);
+        const float2 hb = __half22float2(h);
+        const __half2 l = __floats2half2_rn(a - hb.x, b - hb.y);
+        *reinterpret_cast<__half2 *>(hi + off) = h;
+        *reinterpret_cast<__half2 *>(lo + off) = l;
+    }
+}
+
 // Three-pass FP16 hi/lo product of the A tile (hi at sA, lo at sA + 32 KB)
 // and the B tile (hi at sBh, lo at sBh + NT*256) into TMEM columns [0, NT):
 // D = Ahi Bhi + Ahi Blo + Alo Bhi, K = 128 in eight 16-wide steps.  Issued by
@@ -695,7 +721,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 float v[32];
                 tm_ld32(tmem + lane_base + 256 + c0, v);
 #pragma unroll
-                for (int u = 0; u < 32; ++u) put_split(sBh, sBl, c0 + u, kq, NT, v[u] * s1);
+                for (int u = 0; u < 32; ++u) v[u] *= s1;
+                split_rows32(sBh, sBl, v, c0, kq, lane, NT);
             }
             fence_proxy_async();
             tc_fence_before();
@@ -836,7 +863,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 float v[32];
                 tm_ld32(tmem + lane_base + acc + c0, v);
 #pragma unroll
-                for (int u = 0; u < 32; ++u) put_split(sBh, sBl, c0 + u, kq, NT, v[u] * s2);
+                for (int u = 0; u < 32; ++u) v[u] *= s2;
+                split_rows32(sBh, sBl, v, c0, kq, lane, NT);
             }
             fence_proxy_async();
             tc_fence_before();
