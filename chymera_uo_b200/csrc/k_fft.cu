@@ -68,12 +68,30 @@ struct FftSmem {
     double *rt;        // [nh][2]
 };
 
+// Asynchronous global -> shared copies (bytes = 0: the destination is zeroed;
+// src must still be a valid address).  cp_async_wait_all() then a barrier
+// make them visible to the block.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, int bytes)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Starts the copies of one direction's tables (completed by the caller's
+// cp_async_wait_all + barrier).
 __device__ __forceinline__ void load_fft_tables(const FftDev &f, const FftSmem &s)
 {
-    for (int i = threadIdx.x; i < f.ncompact * 6; i += blockDim.x) s.tw[i] = f.twc[i];
+    for (int i = threadIdx.x; i < f.ncompact * 6; i += blockDim.x) cp_async8(s.tw + i, f.twc + i, 8);
+    for (int i = threadIdx.x; i < f.n; i += blockDim.x) cp_async4(s.perm + i, f.perm + i);
+    for (int i = threadIdx.x; i < 2 * f.nh; i += blockDim.x) cp_async8(s.rt + i, f.rt + i, 8);
     for (int i = threadIdx.x; i < f.ncompact; i += blockDim.x) s.on[i] = f.onc[i];
-    for (int i = threadIdx.x; i < f.n; i += blockDim.x) s.perm[i] = f.perm[i];
-    for (int i = threadIdx.x; i < 2 * f.nh; i += blockDim.x) s.rt[i] = f.rt[i];
 }
 
 template <int L>
@@ -244,15 +262,19 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
     const int j0 = blockIdx.x * T::TC, k = blockIdx.y, b = blockIdx.z;
     const double *rho = bp.rho[b];
 
+    // tables and the tile's samples: every copy in flight at once
     load_fft_tables(t.fwd, fs);
     for (int i = threadIdx.x; i < 20 * (L / 4); i += blockDim.x) {
         const int m = i / (L / 4), l = i % (L / 4);
-        mtab[i] = m < 10 ? t.cosm[(size_t)m * L + l] : t.sinm[(size_t)(m - 10) * L + l];
+        cp_async8(mtab + i, m < 10 ? t.cosm + (size_t)m * L + l : t.sinm + (size_t)(m - 10) * L + l, 8);
     }
     for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
         const int c = i % T::TC, l = i / T::TC, j = j0 + c;
-        A[l * T::RS + c] = (j < t.M) ? rho[(size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] : 0.0;
+        const bool ok = j < t.M;
+        cp_async8(A + l * T::RS + c, ok ? rho + (size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l) : rho,
+                  ok ? 8 : 0);
     }
+    cp_async_wait_all();
     __syncthreads();
 
     // azimuthal moments of each ring (pot/boundary.f:527-538), before DV, using
@@ -411,15 +433,12 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
     // A1(1..N+1) = modes 0..N, B1(2..N) = modes N+1..2N-1, B1(1) = B1(N+1) = 0
     for (int i = threadIdx.x; i < (n + 1) * T::TC; i += blockDim.x) {
         const int c = i % T::TC, q = i / T::TC, j = j0 + c;
-        double re = 0.0, im = 0.0;
-        if (j < t.J) {
-            const size_t col = (size_t)k * t.J + j, pl = (size_t)t.K * t.J;
-            re = X[(size_t)q * pl + col];
-            if (q >= 1 && q < n) im = X[(size_t)(n + q) * pl + col];
-        }
-        A[(2 * q) * T::RS + c] = re;
-        A[(2 * q + 1) * T::RS + c] = im;
+        const bool ok = j < t.J, okim = ok && q >= 1 && q < n;
+        const size_t col = (size_t)k * t.J + j, pl = (size_t)t.K * t.J;
+        cp_async8(A + (2 * q) * T::RS + c, ok ? X + (size_t)q * pl + col : X, ok ? 8 : 0);
+        cp_async8(A + (2 * q + 1) * T::RS + c, okim ? X + (size_t)(n + q) * pl + col : X, okim ? 8 : 0);
     }
+    cp_async_wait_all();
     __syncthreads();
     realtr_pairs<L>(A, fs);
     stages<L, 0, false>(A, fs, t.inv);
