@@ -500,8 +500,8 @@ def main():
         a[...] = b
     for a in pin_p:
         a[...] = 0.0
-    h2d = B * 8 * ((J + 2) * (K + 2) * L + (J + 2) * L + L)
-    d2h = B * 8 * (J + 2) * (K + 2) * L
+    h2d = B * 8 * (J + 2) * (K + 2) * L                      # RHO
+    d2h = B * 8 * L * (K * (J + 2) + (J + 1))                # PHI's write set
     ke = max(3, args.steps // 4)
     for _ in range(args.warmup):
         plan.solve_batch(pin_r, pin_p)

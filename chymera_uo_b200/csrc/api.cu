@@ -412,7 +412,10 @@ static int fetch_diag(chy_plan *p, chy_diag *diag, int nb, int first, cudaStream
 static int ensure_host_staging(chy_plan *p)
 {
     if (p->stage) return CHY_OK;
-    const int c = std::max(1, std::min(std::min(p->max_batch, 4), kMaxBatchPtrs));
+    // one solve per chunk: the copies (two grid volumes over PCIe) take several
+    // times longer than the solve, so small chunks keep the pipeline's fill
+    // and drain short and the solve stays hidden behind the copies
+    const int c = 1;
     const size_t bytes = (size_t)chy_plan::kStageSlots * c * 2 * p->nvol * sizeof(double);
     if (cudaMalloc(&p->stage, bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -438,7 +441,6 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
     if (!p || n < 0 || (n > 0 && (!rho || !phi))) return fail(CHY_ERR_ARG, "null plan or buffers");
     cudaStream_t s = (cudaStream_t)stream;
     const HostPlan &hp = p->hp;
-    const size_t J2 = hp.J + 2, K2 = hp.K + 2, L = hp.L;
     for (int i = 0; i < n; i++)
         if (!rho[i] || !phi[i]) return fail(CHY_ERR_ARG, "null rho/phi pointer");
     if (ptr_kind == CHY_PTR_DEVICE) {
@@ -461,7 +463,7 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
     // Three-stage pipeline over chunks of stage_chunk solves: copy in on
     // s_h2d, solve on the caller's stream, copy out on s_d2h.  A slot is
     // reused only after its previous copy out has finished.
-    const size_t vb = p->nvol * sizeof(double), plane = J2 * K2 * sizeof(double);
+    const size_t vb = p->nvol * sizeof(double);
     // with a host COEF destination, one solve per chunk (COEF is per solve)
     const int c = p->coef_host ? 1 : p->stage_chunk, R = chy_plan::kStageSlots;
     bool used[chy_plan::kStageSlots] = {};
@@ -475,14 +477,7 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         for (int i = 0; i < nb; i++) {
             double *dr = base + (size_t)i * 2 * p->nvol, *df = dr + p->nvol;
             const double *hr = rho[first + i];
-            const double *hf = phi[first + i];
             CHY_CUDA(cudaMemcpyAsync(dr, hr, vb, cudaMemcpyHostToDevice, p->s_h2d));
-            // cells the solve never writes keep the caller's values:
-            // PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :)
-            CHY_CUDA(cudaMemcpy2DAsync(df + J2 * (K2 - 1), plane, hf + J2 * (K2 - 1), plane, J2 * sizeof(double),
-                                       L, cudaMemcpyHostToDevice, p->s_h2d));
-            CHY_CUDA(cudaMemcpy2DAsync(df + (J2 - 1), plane, hf + (J2 - 1), plane, sizeof(double), L,
-                                       cudaMemcpyHostToDevice, p->s_h2d));
             bp.rho[i] = dr;
             bp.phi[i] = df;
         }
@@ -504,7 +499,7 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         CHY_CUDA(cudaEventRecord(p->ev_done[slot], s));
         CHY_CUDA(cudaStreamWaitEvent(p->s_d2h, p->ev_done[slot], 0));
         for (int i = 0; i < nb; i++)
-            CHY_CUDA(cudaMemcpyAsync(phi[first + i], bp.phi[i], vb, cudaMemcpyDeviceToHost, p->s_d2h));
+            CHY_CUDA(copy_phi_write_set(phi[first + i], bp.phi[i], hp.J, hp.K, hp.L, p->s_d2h));
         CHY_CUDA(cudaEventRecord(p->ev_out[slot], p->s_d2h));
         used[slot] = true;
     }

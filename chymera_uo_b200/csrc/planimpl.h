@@ -52,6 +52,19 @@ struct chy_plan {
     MixedState *mx = nullptr;
 };
 
+// Copies the write set of one solve's PHI from device to the caller's host
+// array: PHI(1:JMAX+1, 1, :) and PHI(:, 2:KMAX+1, :).  PHI(:, KMAX+2, :) and
+// PHI(JMAX+2, 1, :) are never written by a solve, so the host keeps its own
+// values there and the device copy never needs them.
+inline cudaError_t copy_phi_write_set(double *host, const double *dev, int J, int K, int L, cudaStream_t s)
+{
+    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2, plane = J2 * K2 * sizeof(double);
+    cudaError_t e = cudaMemcpy2DAsync(host + J2, plane, dev + J2, plane, (size_t)K * J2 * sizeof(double), L,
+                                      cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy2DAsync(host, plane, dev, plane, ((size_t)J + 1) * sizeof(double), L, cudaMemcpyDeviceToHost, s);
+}
+
 // One launch sequence over nb device-pointer solves (api.cu).
 int chy_internal_run_batch(chy_plan *p, const chy::BatchPtrs &bp, int nb, cudaStream_t s);
 

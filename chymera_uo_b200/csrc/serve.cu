@@ -244,7 +244,6 @@ int chy_server::make_class(Request *rq, SizeClass **out)
 // Copies in, solves and copies out the lane's batch on its stream.
 int chy_server::launch(SizeClass &c, Lane &ln)
 {
-    const size_t J2 = c.J + 2, K2 = c.K + 2, L = c.L, plane = J2 * K2 * sizeof(double);
     const size_t vb = c.nvol * sizeof(double);
     BatchPtrs bp{};
     const int nb = (int)ln.batch.size();
@@ -252,19 +251,13 @@ int chy_server::launch(SizeClass &c, Lane &ln)
         Request *rq = ln.batch[i];
         double *dr = reinterpret_cast<double *>(arena_base + rq->buf_off), *df = dr + c.nvol;
         if (cudaMemcpyAsync(dr, rq->rho, vb, cudaMemcpyHostToDevice, ln.stream) != cudaSuccess) return CHY_ERR_CUDA;
-        // cells the solve never writes keep the caller's values
-        if (cudaMemcpy2DAsync(df + J2 * (K2 - 1), plane, rq->phi + J2 * (K2 - 1), plane, J2 * sizeof(double), L,
-                              cudaMemcpyHostToDevice, ln.stream) != cudaSuccess ||
-            cudaMemcpy2DAsync(df + (J2 - 1), plane, rq->phi + (J2 - 1), plane, sizeof(double), L,
-                              cudaMemcpyHostToDevice, ln.stream) != cudaSuccess)
-            return CHY_ERR_CUDA;
         bp.rho[i] = dr;
         bp.phi[i] = df;
     }
     const int st = chy_internal_run_batch(ln.plan, bp, nb, ln.stream);
     if (st != CHY_OK) return st;
     for (int i = 0; i < nb; i++)
-        if (cudaMemcpyAsync(ln.batch[i]->phi, bp.phi[i], vb, cudaMemcpyDeviceToHost, ln.stream) != cudaSuccess)
+        if (copy_phi_write_set(ln.batch[i]->phi, bp.phi[i], c.J, c.K, c.L, ln.stream) != cudaSuccess)
             return CHY_ERR_CUDA;
     if (cudaEventRecord(ln.done, ln.stream) != cudaSuccess) return CHY_ERR_CUDA;
     return CHY_OK;
