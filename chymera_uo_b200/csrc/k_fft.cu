@@ -202,48 +202,6 @@ __device__ __forceinline__ void realtr_pairs(double *A, const FftSmem &s)
     __syncthreads();
 }
 
-// Forward transform of the TC columns held in A (natural sample order): FFT
-// stages, output permutation (in place through registers), REALTR.  Then row
-// 2q holds A1(q+1) and row 2q+1 holds B1(q+1) of pot/pot3.f:99-100, q = 0..N.
-template <int L>
-__device__ __forceinline__ void forward_columns(double *A, const FftSmem &s, const FftDev &f)
-{
-    using T = Tile<L>;
-    constexpr int NI = (T::N + 1) * T::TC, PER = (NI + 255) / 256;
-    stages<L, 0, true>(A, s, f);
-    double re[PER], im[PER];
-#pragma unroll
-    for (int u = 0; u < PER; ++u) {
-        const int w = threadIdx.x + u * 256;
-        if (w < NI) {
-            const int c = w % T::TC, q = w / T::TC;
-            const int src = s.perm[q < T::N ? q : 0];   // A(N+1) = A(1) (pot/fft.f:44-45)
-            re[u] = A[(2 * src) * T::RS + c];
-            im[u] = A[(2 * src + 1) * T::RS + c];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < PER; ++u) {
-        const int w = threadIdx.x + u * 256;
-        if (w < NI) {
-            const int c = w % T::TC, q = w / T::TC;
-            A[(2 * q) * T::RS + c] = re[u];
-            A[(2 * q + 1) * T::RS + c] = im[u];
-        }
-    }
-    __syncthreads();
-    realtr_pairs<L>(A, s);
-}
-
-// Mode l of a transformed column (pot/pot3.f:135-140), before the SF1 scaling.
-template <int L>
-__device__ __forceinline__ double mode_value(const double *A, int l, int c)
-{
-    using T = Tile<L>;
-    return l <= T::N ? A[(2 * l) * T::RS + c] : A[(2 * (l - T::N) + 1) * T::RS + c];
-}
-
 // ---------------------------------------------------------------------------
 // Forward transform of the interior columns + ring moments
 // ---------------------------------------------------------------------------
@@ -297,25 +255,61 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
                 acc[10 + m] = __fma_rn(mtab[(9 + m) * Q + l], (m & 1) ? so : se, acc[10 + m]);
             }
         }
+        // Butterfly reduce-scatter over the column's TPC lanes (21 sums padded
+        // to 32): at each level a lane keeps half of its live sums and adds the
+        // partner's copy of them, so lane g ends with the column totals of
+        // sums base(g) .. base(g) + 32/TPC - 1, in a fixed order.
+        double a[32];
 #pragma unroll
-        for (int q = 0; q < 21; ++q)
+        for (int q = 0; q < 32; ++q) a[q] = q < 21 ? acc[q] : 0.0;
+        int base = 0;
 #pragma unroll
-            for (int o = T::TPC / 2; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        for (int lev = 0; (T::TPC >> (lev + 1)) >= 1; ++lev) {
+            const int o = T::TPC >> (lev + 1), W = 32 >> lev;
+            const bool up = (g & o) != 0;
+#pragma unroll
+            for (int i = 0; i < W / 2; ++i) {
+                const double send = up ? a[i] : a[W / 2 + i];
+                const double keep = up ? a[W / 2 + i] : a[i];
+                a[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+            }
+            base += up ? W / 2 : 0;
+        }
         const int j = j0 + c;
-        if (g == 0 && j < t.M) {
+        if (j < t.M) {
             double *mom = w.mom + (size_t)b * w.smom + (size_t)k * t.M + j;
 #pragma unroll
-            for (int q = 0; q < 21; ++q) mom[(size_t)q * t.nring] = acc[q];
+            for (int i = 0; i < 32 / T::TPC; ++i)
+                if (base + i < 21) mom[(size_t)(base + i) * t.nring] = a[i];
         }
     }
     __syncthreads();
 
-    forward_columns<L>(A, fs, t.fwd);
+    stages<L, 0, true>(A, fs, t.fwd);
 
+    // REALTR (pot/fft.f:2-70) on the transform in natural order -- its sample
+    // q is row perm[q], and A(N+1) = A(1) (pot/fft.f:44-45) -- with the modes
+    // of pot/pot3.f:135-140 written straight to X: A1(q+1) is mode q
+    // (q = 0..N), B1(q+1) mode N+q (q = 1..N-1).  The (j, N-j) pairs are
+    // independent, and each row is read by exactly one pair.
     double *X = w.X + (size_t)b * w.sX;
-    for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
-        const int c = i % T::TC, l = i / T::TC, j = j0 + c;
-        if (j < t.M) X[((size_t)l * t.K + k) * t.J + j] = mode_value<L>(A, l, c) * t.sf1;
+    constexpr int n = T::N, nh = n / 2 + 1;
+    const size_t pl = (size_t)t.K * t.J;
+    for (int i = threadIdx.x; i < nh * T::TC; i += blockDim.x) {
+        const int c = i % T::TC, jp = i / T::TC, kp = n - jp, j = j0 + c;
+        const int sj = fs.perm[jp], sk = fs.perm[kp < n ? kp : 0];
+        const double cn = fs.rt[2 * jp], sn = fs.rt[2 * jp + 1];
+        const double aj = A[(2 * sj) * T::RS + c], bj = A[(2 * sj + 1) * T::RS + c];
+        const double ak = A[(2 * sk) * T::RS + c], bk = A[(2 * sk + 1) * T::RS + c];
+        const double aa = aj + ak, ab = aj - ak, ba = bj + bk, bb = bj - bk;
+        const double re = cn * ba + sn * ab, im = sn * ba - cn * ab;
+        if (j < t.M) {
+            double *xc = X + (size_t)k * t.J + j;
+            xc[(size_t)jp * pl] = (aa + re) * t.sf1;
+            if (jp != kp) xc[(size_t)kp * pl] = (aa - re) * t.sf1;
+            if (jp >= 1) xc[(size_t)(n + jp) * pl] = (im + bb) * t.sf1;
+            if (jp >= 1 && jp != kp) xc[(size_t)(n + kp) * pl] = (im - bb) * t.sf1;
+        }
     }
 }
 
