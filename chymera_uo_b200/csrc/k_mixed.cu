@@ -68,6 +68,7 @@ __host__ __device__ inline uint32_t kmaj_off(int r, int k, int R)
 struct MixedDev {
     const uint8_t *aimg;        // [U hi, U lo, V hi, V lo] swizzled tiles (2^12 scaled)
     const float *lam;           // [128]
+    const float2 *sweep;        // [N+1][ntile][128] {e or f, 1/D} of the radial sweeps
     double *xbuf;               // [nb][L][K][J] FP64 iterate
     size_t sxb;
     double *corr;               // [nb][L][8][2] per mode: sum delta^2, sum x^2
@@ -463,21 +464,16 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
         const int b = (int)(item / t.L), l = (int)(item % t.L);
         const int m = l <= t.N ? l : l - t.N;
         const double xl2 = 2.0 * (t.xlamm[m] - 1.0);
-        // BM_m (pot/pot3.f:226-230) for the FP64 residual, and for the FP32
-        // sweeps the diagonal excess g = BM + AM + CM formed directly (no
-        // cancellation): 2(cos m dtheta - 1) C(j), plus the axis term at j = 0
-        // and -CMMAX at j = M-1
+        // BM_m (pot/pot3.f:226-230) for the FP64 residual (the sweeps use the
+        // tabulated multipliers)
         for (int j = tid; j < 256; j += blockDim.x) {
-            double bm = 0.0, gm = 0.0;
+            double bm = 0.0;
             if (j < M) {
                 const double axis = (((m & 1) ? -1.0 : 1.0) - 1.0) * t.ammin;
                 bm = t.bm0[j] + xl2 * t.cc[j];
-                gm = xl2 * t.cc[j];
-                if (j == 0) { bm = t.bm0[0] + axis + xl2 * t.cc[0]; gm = axis + gm; }
-                if (j == M - 1) gm = gm - t.cmmax;
+                if (j == 0) bm = t.bm0[0] + axis + xl2 * t.cc[0];
             }
             d_bm[j] = bm;
-            f_t[j].x = (float)gm;
         }
         double *Xl = w.X + (size_t)b * w.sX + (size_t)l * K * J;
         double *xl = kRes ? nullptr : x.xbuf + (size_t)b * x.sxb + (size_t)l * K * J;
@@ -738,71 +734,57 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 bulk_g2s(sA, x.aimg + kAImg, kAImg, bar_a);
             }
             a_inflight = true;
-            // ---- radial sweeps (T_r(m) + lam_p) w = W_p, top-down and bottom-up
-            // halves.  The multipliers go to shared memory (the B tile is free
-            // until the next split): cvs[j][p].
+            // ---- radial sweeps (T_r(m) + lam_p) w = W_p, top-down over rows
+            // [0, h) and bottom-up over [h, M), meeting in the middle.  The
+            // multipliers and pivot reciprocals come from the sweep table, so
+            // each row costs one dependent FMA; the table loads of a chunk are
+            // independent of the recurrence and issue ahead of it.
             float xmax = 0.0f;
             {
-                float *cvs = reinterpret_cast<float *>(sBh);
                 const int p = kq;
                 const bool live = p < NZ;
-                const float lam = f_lam[p];
-                const int h = 32 * ((M + 63) / 64);   // rows [0,h) top, [h,M) bottom; M >= 63
+                const int h = 32 * ((M + 63) / 64);   // M >= 63, h < M, h % 32 == 0
                 const uint32_t tb = tmem + lane_base + acc;
+                const float2 *sw = x.sweep + (size_t)m * NT * 128 + p;   // row j at sw[j * 128]
+                float *cvs = reinterpret_cast<float *>(sBh);   // [j][p] multipliers for the back sweeps
                 float yv[32];
-                // Elimination in excess form: with g = d + a + c (the small
-                // diagonal excess) the top-down multipliers c' = c/D are kept as
-                // e = 1 + c' = (g - a e_prev)/D, D = (g - a e_prev) - c, so no
-                // near-cancelling sum is formed in FP32; bottom-up likewise with
-                // f = 1 + a''.
-                // The loops are branch-free (h is a multiple of 32 and h < M):
-                // rows outside [0, M) and padding lanes (p >= NZ) compute
-                // values that are discarded by selects, so the coefficient
-                // loads of a chunk can all be issued ahead of the recurrence.
-                float cv[32];
+                float2 T[32];
                 if (jh == 0) {
-                    float e = 0.f, yp = 0.f;
+                    float yp = 0.f;
                     for (int c0 = 0; c0 < h; c0 += 32) {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) T[u] = sw[(size_t)(c0 + u) * 128];
                         tm_ld32(tb + c0, yv);
 #pragma unroll
                         for (int u = 0; u < 32; ++u) {
-                            const float4 T = f_t[c0 + u];
-                            const float tt = (T.x + lam) - T.y * e;
-                            const float rr = __fdividef(1.0f, tt - T.z);
-                            e = tt * rr;
-                            yp = (yv[u] - T.y * yp) * rr;
+                            const float rr = T[u].y, ar = f_t[c0 + u].y * rr;
+                            yp = fmaf(-ar, yp, yv[u] * rr);
                             yv[u] = yp;
-                            cv[u] = e;
                         }
                         tm_st32_nw(tb + c0, yv);
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) cvs[(c0 + u) * 128 + p] = cv[u];
+                        for (int u = 0; u < 32; ++u) cvs[(c0 + u) * 128 + p] = T[u].x;
                     }
                     f_xch[p * 4 + 0] = yp;
-                    f_xch[p * 4 + 1] = e;
                 } else {
-                    float f = 0.f, yp = 0.f;
+                    float yp = 0.f;
                     const int cl = ((M - 1) / 32) * 32;
                     for (int c0 = cl; c0 >= h; c0 -= 32) {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) T[u] = sw[(size_t)(c0 + u) * 128];
                         tm_ld32(tb + c0, yv);
 #pragma unroll
                         for (int u = 31; u >= 0; --u) {
-                            const bool in = c0 + u < M;   // uniform
-                            const float4 T = f_t[c0 + u];
-                            const float tt = (T.x + lam) - T.z * f;
-                            const float rr = __fdividef(1.0f, tt - T.y);
-                            const float fn = tt * rr, yn = (yv[u] - T.z * yp) * rr;
-                            f = in ? fn : f;
-                            yp = in ? yn : yp;
+                            const float rr = T[u].y, cr = f_t[c0 + u].z * rr;
+                            const float yn = fmaf(-cr, yp, yv[u] * rr);
+                            yp = (c0 + u < M) ? yn : yp;   // uniform
                             yv[u] = yn;
-                            cv[u] = fn;
                         }
                         tm_st32_nw(tb + c0, yv);
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) cvs[(c0 + u) * 128 + p] = cv[u];
+                        for (int u = 0; u < 32; ++u) cvs[(c0 + u) * 128 + p] = T[u].x;
                     }
                     f_xch[p * 4 + 2] = yp;
-                    f_xch[p * 4 + 3] = f;
                 }
                 tm_wait_st();
                 __syncthreads();
@@ -810,20 +792,20 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 // x_t = y'_t + (1-e_t) x_u, x_u = y''_u + (1-f_u) x_t
                 float xt, xu;
                 {
-                    const float yt = f_xch[p * 4 + 0], et = f_xch[p * 4 + 1];
-                    const float yu = f_xch[p * 4 + 2], fu = f_xch[p * 4 + 3];
+                    const float yt = f_xch[p * 4 + 0], et = cvs[(h - 1) * 128 + p];
+                    const float yu = f_xch[p * 4 + 2], fu = cvs[h * 128 + p];
                     xt = (yt + (1.0f - et) * yu) / ((et + fu) - et * fu);
                     xu = yu + (1.0f - fu) * xt;
                 }
                 if (jh == 0) {
                     float xn = xt;   // x_{j+1} while sweeping up
                     for (int c0 = h - 32; c0 >= 0; c0 -= 32) {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) T[u].x = cvs[(c0 + u) * 128 + p];
                         tm_ld32(tb + c0, yv);
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) cv[u] = cvs[(c0 + u) * 128 + p];
-#pragma unroll
                         for (int u = 31; u >= 0; --u) {
-                            float xv = yv[u] + (1.0f - cv[u]) * xn;
+                            float xv = yv[u] + (1.0f - T[u].x) * xn;
                             xv = (c0 + u == h - 1) ? xt : xv;
                             xn = xv;
                             yv[u] = live ? xv : 0.f;
@@ -834,12 +816,12 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 } else {
                     float xp = xu;   // x_{j-1} while sweeping down
                     for (int c0 = h; c0 < NT; c0 += 32) {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) T[u].x = cvs[(c0 + u) * 128 + p];
                         tm_ld32(tb + c0, yv);
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) cv[u] = cvs[(c0 + u) * 128 + p];
-#pragma unroll
                         for (int u = 0; u < 32; ++u) {
-                            float xv = yv[u] + (1.0f - cv[u]) * xp;
+                            float xv = yv[u] + (1.0f - T[u].x) * xp;
                             xv = (c0 + u == h) ? xu : xv;
                             xp = xv;
                             yv[u] = (live && c0 + u < M) ? xv : 0.f;
@@ -1012,6 +994,50 @@ bool chy_mixed_supported(const chy::HostPlan *hp)
     return hp->NZ <= 127 && hp->J >= 64 && hp->J % 16 == 0 && round64(hp->J) <= kMaxN;
 }
 
+// Radial sweep table: for every azimuthal index m = 0..N and vertical
+// eigenvalue p (padding rows use -1), the multipliers of the two-sided
+// elimination of (T_r(m) + lam_p) in excess form and the pivot reciprocals,
+// {e_j or f_j, 1/D_j} as FP32 pairs, layout [m][j][p] (j < ntile, p < 128).
+// Rows [0, h) are eliminated top-down, rows [h, M) bottom-up,
+// h = 32 ceil(M / 64).  They do not depend on the data, so they are formed
+// once, in FP64, here.
+static std::vector<float> sweep_table(const chy::HostPlan &hp)
+{
+    const int M = hp.M, NT = round64(hp.J), n = hp.N, h = 32 * ((M + 63) / 64);
+    std::vector<float> t((size_t)(n + 1) * NT * 128 * 2, 0.0f);
+    std::vector<double> g(M);
+    for (int m = 0; m <= n; ++m) {
+        const double xl2 = 2.0 * (hp.xlamm[m] - 1.0);
+        const double axis = (((m & 1) ? -1.0 : 1.0) - 1.0) * hp.ammin;
+        for (int j = 0; j < M; ++j) {
+            g[j] = xl2 * hp.cc[j];
+            if (j == 0) g[j] = axis + g[j];
+            if (j == M - 1) g[j] = g[j] - hp.cmmax;
+        }
+        for (int p = 0; p < 128; ++p) {
+            const double lam = p < hp.NZ ? hp.lam[p] : -1.0;
+            auto put = [&](int j, double c, double r) {
+                float *q = &t[(((size_t)m * NT + j) * 128 + p) * 2];
+                q[0] = (float)c;
+                q[1] = (float)r;
+            };
+            double e = 0.0;
+            for (int j = 0; j < h; ++j) {
+                const double tt = (g[j] + lam) - hp.am[j] * e, rr = 1.0 / (tt - hp.cm[j]);
+                e = tt * rr;
+                put(j, e, rr);
+            }
+            double f = 0.0;
+            for (int j = M - 1; j >= h; --j) {
+                const double tt = (g[j] + lam) - hp.cm[j] * f, rr = 1.0 / (tt - hp.am[j]);
+                f = tt * rr;
+                put(j, f, rr);
+            }
+        }
+    }
+    return t;
+}
+
 size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image)
 {
     // [U hi | U lo | V hi | V lo]: K-major swizzled FP16 tiles of 2^12 * U(p,k)
@@ -1041,7 +1067,13 @@ size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image)
     size_t off2 = (image->size() + 255) & ~(size_t)255;
     image->resize(off2 + lam.size() * sizeof(float));
     std::memcpy(image->data() + off2, lam.data(), lam.size() * sizeof(float));
-    return off;   // lam follows at the next 256-byte boundary after the tiles
+    // radial sweep coefficients, then the sweep table at the next 256-byte
+    // boundary
+    const std::vector<float> sw = sweep_table(*hp);
+    size_t off3 = (image->size() + 255) & ~(size_t)255;
+    image->resize(off3 + sw.size() * sizeof(float));
+    std::memcpy(image->data() + off3, sw.data(), sw.size() * sizeof(float));
+    return off;   // lam and the sweep table follow at 256-byte boundaries
 }
 
 void chy_mixed_bind_tables(chy_plan *p, char *dev_base)
@@ -1050,6 +1082,8 @@ void chy_mixed_bind_tables(chy_plan *p, char *dev_base)
     p->mx->dev.aimg = reinterpret_cast<const uint8_t *>(dev_base);
     size_t lam_off = (((size_t)(dev_base - p->d_tables) + 2 * kAImg) + 255) & ~(size_t)255;
     p->mx->dev.lam = reinterpret_cast<const float *>(p->d_tables + lam_off);
+    const size_t sw_off = (lam_off + 128 * sizeof(float) + 255) & ~(size_t)255;
+    p->mx->dev.sweep = reinterpret_cast<const float2 *>(p->d_tables + sw_off);
 }
 
 // Per-mode correction sums and the error word; the FP64 iterate of the
