@@ -116,65 +116,113 @@ __device__ __forceinline__ FftSmem carve_fft(char *p)
     return s;
 }
 
-// One decimation stage S of pot/fft.f FFT on the TC columns of A, then the
-// following stages.
+// One butterfly of pot/fft.f's radix-2 or radix-4 step on values held in
+// registers, in the reference's operation order (compiled without FMA
+// contraction, so every product and sum rounds as there).  tw: the recorded
+// rotations of this position, on: whether they apply.
+template <int R, bool FWD>
+__device__ __forceinline__ void butterfly(double &a0, double &b0, double &a1, double &b1, double &a2, double &b2,
+                                          double &a3, double &b3, bool on, const double *tw)
+{
+    if constexpr (R == 2) {
+        if (!on) {
+            const double ak = a1, bk = b1;
+            a1 = a0 - ak;
+            b1 = b0 - bk;
+            a0 = a0 + ak;
+            b0 = b0 + bk;
+        } else {
+            const double c1 = tw[0], s1 = tw[1];
+            const double ak = a0 - a1, bk = b0 - b1;
+            a0 = a0 + a1;
+            b0 = b0 + b1;
+            a1 = c1 * ak - s1 * bk;
+            b1 = s1 * ak + c1 * bk;
+        }
+    } else {
+        double akp = a0 + a2, akm = a0 - a2, ajp = a1 + a3, ajm = a1 - a3;
+        const double A0 = akp + ajp;
+        ajp = akp - ajp;
+        double bkp = b0 + b2, bkm = b0 - b2, bjp = b1 + b3, bjm = b1 - b3;
+        const double B0 = bkp + bjp;
+        bjp = bkp - bjp;
+        if constexpr (FWD) {
+            akp = akm - bjm; akm = akm + bjm; bkp = bkm + ajm; bkm = bkm - ajm;
+        } else {
+            akp = akm + bjm; akm = akm - bjm; bkp = bkm - ajm; bkm = bkm + ajm;
+        }
+        a0 = A0;
+        b0 = B0;
+        if (on) {
+            a1 = akp * tw[0] - bkp * tw[1]; b1 = akp * tw[1] + bkp * tw[0];
+            a2 = ajp * tw[2] - bjp * tw[3]; b2 = ajp * tw[3] + bjp * tw[2];
+            a3 = akm * tw[4] - bkm * tw[5]; b3 = akm * tw[5] + bkm * tw[4];
+        } else {
+            a1 = akp; b1 = bkp; a2 = ajp; b2 = bjp; a3 = akm; b3 = bkm;
+        }
+    }
+}
+
+// Stages S and S+1 of the transform in one pass over shared memory (S alone
+// when it is the last).  Stage S+1 works inside the blocks of stage S, so the
+// R_S * R_{S+1} elements base + i H_{S+1} of a group are closed under both
+// stages: a thread loads them, applies stage S's R_{S+1} butterflies and then
+// stage S+1's R_S butterflies in registers, and stores them back.  Each
+// butterfly is the one the element-by-element stage loop would apply.
 template <int L, int S, bool FWD>
-__device__ __forceinline__ void stages(double *A, const FftSmem &s, const FftDev &f)
+__device__ __forceinline__ void stage_pairs(double *A, const FftSmem &s, const FftDev &f)
 {
     using T = Tile<L>;
     using Sh = Shape<T::N>;
     if constexpr (S < Sh::nst()) {
-        constexpr int R = Sh::radix(S), H = Sh::span(S), NBF = T::N / R;
-        const int off = f.off[S];
-        for (int w = threadIdx.x; w < NBF * T::TC; w += blockDim.x) {
-            const int c = w % T::TC, bi = w / T::TC;
-            const int j = bi % H, kk = (bi / H) * (R * H) + j;
-            const bool on = s.on[off + j] != 0;
-            const double *tw = s.tw + (size_t)(off + j) * 6;
-            double *a0 = A + (2 * kk) * T::RS + c, *b0 = a0 + T::RS;
-            double *a1 = A + (2 * (kk + H)) * T::RS + c, *b1 = a1 + T::RS;
-            if constexpr (R == 2) {
-                if (!on) {
-                    const double ak = *a1, bk = *b1;
-                    *a1 = *a0 - ak;
-                    *b1 = *b0 - bk;
-                    *a0 = *a0 + ak;
-                    *b0 = *b0 + bk;
-                } else {
-                    const double c1 = tw[0], s1 = tw[1];
-                    const double ak = *a0 - *a1, bk = *b0 - *b1;
-                    *a0 = *a0 + *a1;
-                    *b0 = *b0 + *b1;
-                    *a1 = c1 * ak - s1 * bk;
-                    *b1 = s1 * ak + c1 * bk;
+        constexpr bool two = S + 1 < Sh::nst();
+        constexpr int R1 = Sh::radix(S), H1 = Sh::span(S);
+        constexpr int R2 = two ? Sh::radix(S + 1) : 1, H2 = two ? Sh::span(S + 1) : H1;
+        constexpr int G = R1 * R2, NG = T::N / G;
+        const int off1 = f.off[S], off2 = two ? f.off[S + 1] : 0;
+        for (int w = threadIdx.x; w < NG * T::TC; w += blockDim.x) {
+            const int c = w % T::TC, gi = w / T::TC;
+            const int j = gi % H2, base = (gi / H2) * (R1 * H1) + j;
+            double re[G], im[G];
+#pragma unroll
+            for (int i = 0; i < G; ++i) {
+                re[i] = A[(2 * (base + i * H2)) * T::RS + c];
+                im[i] = A[(2 * (base + i * H2) + 1) * T::RS + c];
+            }
+            // stage S: butterflies m = 0..R2-1 on elements m + t R2 (t < R1)
+#pragma unroll
+            for (int m = 0; m < R2; ++m) {
+                const int js = j + m * H2;
+                const bool on = s.on[off1 + js] != 0;
+                const double *tw = s.tw + (size_t)(off1 + js) * 6;
+                if constexpr (R1 == 2)
+                    butterfly<2, FWD>(re[m], im[m], re[m + R2], im[m + R2], re[m], im[m], re[m], im[m], on, tw);
+                else
+                    butterfly<4, FWD>(re[m], im[m], re[m + R2], im[m + R2], re[m + 2 * R2], im[m + 2 * R2],
+                                      re[m + 3 * R2], im[m + 3 * R2], on, tw);
+            }
+            if constexpr (two) {
+                // stage S+1: butterflies t = 0..R1-1 on elements t R2 + m' (m' < R2)
+                const bool on = s.on[off2 + j] != 0;
+                const double *tw = s.tw + (size_t)(off2 + j) * 6;
+#pragma unroll
+                for (int t = 0; t < R1; ++t) {
+                    const int e = t * R2;
+                    if constexpr (R2 == 2)
+                        butterfly<2, FWD>(re[e], im[e], re[e + 1], im[e + 1], re[e], im[e], re[e], im[e], on, tw);
+                    else
+                        butterfly<4, FWD>(re[e], im[e], re[e + 1], im[e + 1], re[e + 2], im[e + 2], re[e + 3],
+                                          im[e + 3], on, tw);
                 }
-            } else {
-                double *a2 = A + (2 * (kk + 2 * H)) * T::RS + c, *b2 = a2 + T::RS;
-                double *a3 = A + (2 * (kk + 3 * H)) * T::RS + c, *b3 = a3 + T::RS;
-                double akp = *a0 + *a2, akm = *a0 - *a2, ajp = *a1 + *a3, ajm = *a1 - *a3;
-                const double A0 = akp + ajp;
-                ajp = akp - ajp;
-                double bkp = *b0 + *b2, bkm = *b0 - *b2, bjp = *b1 + *b3, bjm = *b1 - *b3;
-                const double B0 = bkp + bjp;
-                bjp = bkp - bjp;
-                if constexpr (FWD) {
-                    akp = akm - bjm; akm = akm + bjm; bkp = bkm + ajm; bkm = bkm - ajm;
-                } else {
-                    akp = akm + bjm; akm = akm - bjm; bkp = bkm - ajm; bkm = bkm + ajm;
-                }
-                *a0 = A0;
-                *b0 = B0;
-                if (on) {
-                    *a1 = akp * tw[0] - bkp * tw[1]; *b1 = akp * tw[1] + bkp * tw[0];
-                    *a2 = ajp * tw[2] - bjp * tw[3]; *b2 = ajp * tw[3] + bjp * tw[2];
-                    *a3 = akm * tw[4] - bkm * tw[5]; *b3 = akm * tw[5] + bkm * tw[4];
-                } else {
-                    *a1 = akp; *b1 = bkp; *a2 = ajp; *b2 = bjp; *a3 = akm; *b3 = bkm;
-                }
+            }
+#pragma unroll
+            for (int i = 0; i < G; ++i) {
+                A[(2 * (base + i * H2)) * T::RS + c] = re[i];
+                A[(2 * (base + i * H2) + 1) * T::RS + c] = im[i];
             }
         }
         __syncthreads();
-        stages<L, S + 1, FWD>(A, s, f);
+        stage_pairs<L, two ? S + 2 : S + 1, FWD>(A, s, f);
     }
 }
 
@@ -285,7 +333,7 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
     }
     __syncthreads();
 
-    stages<L, 0, true>(A, fs, t.fwd);
+    stage_pairs<L, 0, true>(A, fs, t.fwd);
 
     // REALTR (pot/fft.f:2-70) on the transform in natural order -- its sample
     // q is row perm[q], and A(N+1) = A(1) (pot/fft.f:44-45) -- with the modes
@@ -435,7 +483,7 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
     cp_async_wait_all();
     __syncthreads();
     realtr_pairs<L>(A, fs);
-    stages<L, 0, false>(A, fs, t.inv);
+    stage_pairs<L, 0, false>(A, fs, t.inv);
 
     // sample l of column c in natural order, times SF2 = 0.5 (pot/pot3.f:276-279)
     auto sample = [&](int l, int c) -> double {
