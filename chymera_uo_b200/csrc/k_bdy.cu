@@ -13,47 +13,51 @@
 // The outside sums are accumulated from the outermost ring inward, so the
 // huge r^-(2l+1) factors of inner rings never enter a difference.
 //
-// Compiled with --fmad=false so the ring terms equal the host tables bitwise.
+// Compiled with --fmad=false: each product and sum rounds separately, in a
+// fixed order.
 #include "devplan.h"
-#include "legendre.h"
 
 namespace chy {
 
-__constant__ LegTerm c_leg[66] = CHY_LEG_TABLE;
-
-// Grid: (nsub, 1, batch), 256 threads.
-__global__ void __launch_bounds__(256) k_bdy_sub(DevTables t, Work w)
+// Grid: (nsub, 1, ceil(batch / kSubBatch)), 256 threads.  The ring-table
+// slice of a sub-chunk is loaded once and serves up to kSubBatch solves.
+constexpr int kSubBatch = 8;
+__global__ void __launch_bounds__(256) k_bdy_sub(DevTables t, Work w, int nb)
 {
     extern __shared__ double smem[];
     const int RL = t.srow, NT_ = t.ntrm;
     double *s_row = smem;                                      // [ns][RL]: TERM, r^-(2l+1), DV
     double (*s_mom)[21] = reinterpret_cast<double (*)[21]>(smem + kSubChunk * RL);
-    const int sc = blockIdx.x, b = blockIdx.z;
+    const int sc = blockIdx.x;
     const int s0 = t.sub_start[sc], s1 = t.sub_start[sc + 1], ns = s1 - s0;
-    const double *mom = w.mom + (size_t)b * w.smom;
 
     // per ring, geometry from the plan (TERM(I) of pot/boundary.f:385-502,
-    // r^-(2l+1) of :587, DV of :516) and DV * moments from this solve
+    // r^-(2l+1) of :587, DV of :516)
     for (int i = threadIdx.x; i < ns * RL; i += blockDim.x) s_row[i] = t.sterm[(size_t)s0 * RL + i];
-    __syncthreads();
-    for (int it = threadIdx.x; it < ns * 21; it += blockDim.x) {
-        const int r = it / 21, q = it % 21;
-        s_mom[r][q] = s_row[r * RL + NT_ + 11] * mom[(size_t)q * t.nring + t.ring_sorted[s0 + r]];
-    }
-    __syncthreads();
-
-    double *sub = w.sub + (size_t)b * w.ssub + (size_t)sc * 2 * t.ncol;
-    for (int cc = threadIdx.x; cc < 2 * t.ncol; cc += blockDim.x) {
-        const int col = cc % t.ncol, out = cc / t.ncol;
-        const int term = t.col_term[col], m = t.col_m[col], l = t.col_l[col];
-        const int mq = t.col_part[col] == 0 ? m : 10 + m;
-        double acc = 0.0;
-        if (!out) {
-            for (int r = 0; r < ns; ++r) acc = acc + s_row[r * RL + term] * s_mom[r][mq];
-        } else {
-            for (int r = 0; r < ns; ++r) acc = acc + (s_row[r * RL + term] * s_mom[r][mq]) * s_row[r * RL + NT_ + l];
+    const int b0 = blockIdx.z * kSubBatch, b1 = min(nb, b0 + kSubBatch);
+    for (int b = b0; b < b1; ++b) {
+        __syncthreads();   // s_row loaded / s_mom of the previous solve consumed
+        // DV * moments of this solve
+        const double *mom = w.mom + (size_t)b * w.smom;
+        for (int it = threadIdx.x; it < ns * 21; it += blockDim.x) {
+            const int r = it / 21, q = it % 21;
+            s_mom[r][q] = s_row[r * RL + NT_ + 11] * mom[(size_t)q * t.nring + t.ring_sorted[s0 + r]];
         }
-        sub[(size_t)out * t.ncol + col] = acc;
+        __syncthreads();
+        double *sub = w.sub + (size_t)b * w.ssub + (size_t)sc * 2 * t.ncol;
+        for (int cc = threadIdx.x; cc < 2 * t.ncol; cc += blockDim.x) {
+            const int col = cc % t.ncol, out = cc / t.ncol;
+            const int term = t.col_term[col], m = t.col_m[col], l = t.col_l[col];
+            const int mq = t.col_part[col] == 0 ? m : 10 + m;
+            double acc = 0.0;
+            if (!out) {
+                for (int r = 0; r < ns; ++r) acc = acc + s_row[r * RL + term] * s_mom[r][mq];
+            } else {
+                for (int r = 0; r < ns; ++r)
+                    acc = acc + (s_row[r * RL + term] * s_mom[r][mq]) * s_row[r * RL + NT_ + l];
+            }
+            sub[(size_t)out * t.ncol + col] = acc;
+        }
     }
 }
 
@@ -112,7 +116,7 @@ cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStrea
     const size_t sm = (size_t)kSubChunk * (t.srow + 21) * sizeof(double);
     cudaError_t e = ensure_smem((const void *)k_bdy_sub, sm);
     if (e != cudaSuccess) return e;
-    k_bdy_sub<<<dim3(t.nsub, 1, nb), 256, sm, s>>>(t, w);
+    k_bdy_sub<<<dim3(t.nsub, 1, (nb + kSubBatch - 1) / kSubBatch), 256, sm, s>>>(t, w, nb);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_bdy_scan<<<dim3(2 * t.ncol, 1, nb), 256, 0, s>>>(t, w);
