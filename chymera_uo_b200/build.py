@@ -3,7 +3,8 @@
     python -m chymera_uo_b200.build [--force] [--verbose]
 
 Objects go to chymera_uo_b200/_build/, the library to
-chymera_uo_b200/libchy_pot3.so.  Transform and boundary kernels are compiled
+chymera_uo_b200/libchy_pot3.so, the ITYPE=71 driver to
+chymera_uo_b200/chy_itype71.  Transform and boundary kernels are compiled
 with --fmad=false (their products and sums must round like the reference's);
 host code with -ffp-contract=off for the same reason.
 """
@@ -21,6 +22,7 @@ CSRC = os.path.join(HERE, "csrc")
 INC = os.path.join(ROOT, "include")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libchy_pot3.so")
+CLI = os.path.join(HERE, "chy_itype71")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
@@ -80,6 +82,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
         _run(cmd, verbose)
     if force or _stale(LIB, objs):
         _run([nvcc()] + ARCH + ["-shared", "-o", LIB] + objs, verbose)
+    # the ITYPE=71 driver, linked against the library next to it
+    cli_src = os.path.join(CSRC, "cli", "itype71.cpp")
+    if force or _stale(CLI, [cli_src, LIB] + hdrs):
+        _run(["g++"] + CXX_FLAGS + [cli_src, "-o", CLI, "-L" + HERE, "-lchy_pot3", "-Wl,-rpath,$ORIGIN"], verbose)
     return LIB
 
 
