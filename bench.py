@@ -57,6 +57,43 @@ def host_threads():
 
 
 # ---------------------------------------------------------------- helpers
+# Replicas: every rank solves its own densities; the only collectives are the
+# barriers around the timed region and the max of the ranks' times.
+def init_replicas(ws, local, backend="nccl", timeout_s=120):
+    """The process group for ws > 1 ranks (None for one rank)."""
+    if ws <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+    return dist
+
+
+def replica_barrier(dist, device):
+    import torch
+    if dist is not None:
+        dist.barrier()
+    if device == "cuda":
+        torch.cuda.synchronize()
+
+
+def replica_max(dist, x, device):
+    """Max of x over the ranks (the slowest rank's time)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ws, solves_per_rank_step, steps, ms_max):
+    """Whole-job solves/s: all ranks' solves over the slowest rank's time."""
+    return ws * solves_per_rank_step * steps / (ms_max * 1e-3)
+
+
 def dist_info():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), ws
@@ -205,7 +242,7 @@ def run_batch_workload(args):
     """64 seeded disks of uneven sizes (JMAX in {64,128,256}, KMAX in
     {32,64,128}, LMAX in {64,128,256}, random slope and H/r): one step = one
     replay of a CUDA graph holding chy_solve_multi over all of them; the FP64
-    path is timed the same way.  Single GPU (replicas as for pot3)."""
+    path is timed the same way.  One GPU (the rank-0 device)."""
     import torch
     import chymera_uo_b200 as chy
     from chymera_uo_b200 import synth
@@ -386,24 +423,13 @@ def main():
 
     rank, local, ws = dist_info()
     torch.cuda.set_device(local)
-    dist = None
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = init_replicas(ws, local)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replica_barrier(dist, "cuda")
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_max(dist, x, "cuda")
 
     B = args.batch
     host = densities(B, rank * B)
@@ -435,7 +461,7 @@ def main():
     stage, calls = plan.stage_times()
     plan.set_profiling(False)
     clocks = clk.summary()
-    value = ws * B * args.steps / (ms * 1e-3)
+    value = replica_value(ws, B, args.steps, ms)
 
     # ---- dominant kernel: the mode solves (one launch per step)
     mode_ms = stage["mode solves"] / max(calls, 1)
