@@ -400,6 +400,8 @@ def main():
     ap.add_argument("--batch", type=int, default=32, help="solves per step (launch sequence)")
     ap.add_argument("--impl", default="chymera", choices=["chymera", "reference"])
     ap.add_argument("--refine", type=int, default=1, help="mixed-precision refinement corrections")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="mode-solve path of the timed plan (fp64: the plain FP64 GPU path)")
     ap.add_argument("--latency-samples", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -437,8 +439,9 @@ def main():
     phis = [chy.fortran_zeros_cuda((J + 2, K + 2, L)) for _ in range(B)]
     ref_phis = [chy.fortran_zeros_cuda((J + 2, K + 2, L)) for _ in range(B)]
     g = chy.grid(J, K, L)
-    plan = chy.Plan(g, "mixed", B)
-    plan.set_refine(args.refine)
+    plan = chy.Plan(g, args.precision, B)
+    if args.precision == "mixed":
+        plan.set_refine(args.refine)
     plan64 = chy.Plan(g, "fp64", B)
     stream = torch.cuda.current_stream()
 
@@ -468,8 +471,9 @@ def main():
     alg = mode_solve_bytes_per_solve() * B
     hbm, peak_kind = peaks()
     achieved = alg / (mode_ms * 1e-3) / 1e9
-    tps = profiled_traffic_per_solve()
-    roofline = {"bound": "hbm", "kernel": "k_mode_mixed", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+    tps = profiled_traffic_per_solve() if args.precision == "mixed" else None
+    kname = "k_mode_mixed" if args.precision == "mixed" else "FP64 mode solves (k_zfwd_f64, k_thomas_f64, k_zinv_f64)"
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
                 "traffic": None if tps is None else tps * B,
                 "algorithmic_bytes": alg, "launch_ms": mode_ms,
@@ -560,9 +564,11 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "mixed: f16 hi/lo tensor-core + f32 + f64",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "mixed: f16 hi/lo tensor-core + f32 + f64" if args.precision == "mixed" else "f64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "jmax": J, "kmax": K, "lmax": L, "solves_per_step": B,
+                "config": {"workload": WORKLOAD if args.precision == "mixed" else
+                           WORKLOAD.replace("mixed precision", "plain FP64 GPU path"), "jmax": J, "kmax": K, "lmax": L, "solves_per_step": B,
                            "refine_corrections": args.refine, "parallelism": f"replicas x{ws}",
                            "l2": f"inputs larger than L2 ({B} x {8 * (J + 2) * (K + 2) * L / 1e6:.0f} MB "
                                  "RHO + PHI resident)"},
