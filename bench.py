@@ -304,6 +304,109 @@ def run_batch_workload(args):
     return 0
 
 
+# ---------------------------------------------------------------- time-step workload
+STAR = dict(mass_star=1.0, tmassacc=0.0125, rpstar=0.0031, phi_star=0.7)
+
+
+def source_bytes_per_launch(jh=J, kh=K, jmin=2):
+    """Algorithmic HBM bytes of one SOURCE launch: per updated cell
+    (J = JSTART..JMAX+1, K = 2..KMAX+1, every L) it reads RHO, PHI, OMEGA, P,
+    S, T, A once and writes S, T, A once, 10 x 8 bytes."""
+    jstart = max(jmin, 2)
+    return 80 * (jh + 2 - jstart) * kh * L
+
+
+def run_step_workload(args):
+    """The gravity of one hydro time step at 256x128x256, in the reference's
+    order (radhydro/3dhyd-main.f:474-524): BDYGEN + POT3, ExternalPot (fused
+    into the inverse transform), then SOURCE's potential, pressure and
+    rotation terms.  One solve per step, as the reference does; device
+    arrays.  Reports steps/s, the inverse transform with and without the star
+    potential, and the SOURCE kernel against the HBM roofline."""
+    import torch
+    import chymera_uo_b200 as chy
+    rank, local, ws = dist_info()
+    torch.cuda.set_device(local)
+    rho = chy.to_cuda_fortran(densities(1, rank)[0])
+    phi = chy.fortran_zeros_cuda((J + 2, K + 2, L))
+    rng = np.random.default_rng(5 + rank)
+    hyd = {k: chy.to_cuda_fortran(np.asfortranarray(rng.random((J + 2, K + 2, L)))) for k in
+           ("omega", "p", "s", "t", "a")}
+    g = chy.grid(J, K, L)
+    plan = chy.Plan(g, args.precision, 1)
+    plan.set_external(**STAR)
+    bare = chy.Plan(g, args.precision, 1)
+    stream = torch.cuda.current_stream()
+    delt = 1e-6
+
+    def step(p, with_source=True):
+        p.solve(rho, phi)
+        if with_source:
+            p.source(rho, phi, hyd["omega"], hyd["p"], hyd["s"], hyd["t"], hyd["a"], delt)
+
+    for _ in range(args.warmup):
+        step(plan)
+        step(bare, False)
+    torch.cuda.synchronize()
+    # whole steps
+    launches0 = plan.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(plan)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    gpu_launches = plan.launches - launches0
+    # stage times with and without the star potential
+    inv = {}
+    for name, p in (("with_star", plan), ("without_star", bare)):
+        p.set_profiling(True)
+        for _ in range(args.steps):
+            p.solve(rho, phi)
+        torch.cuda.synchronize()
+        st, calls = p.stage_times()
+        p.set_profiling(False)
+        inv[name] = st["inverse+ghosts+zaxphi"] / max(calls, 1)
+    # SOURCE alone: right after a solve (PHI partly in L2) and after an L2 flush
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    src = {}
+    for name, flush_first in (("after_solve", False), ("after_l2_flush", True)):
+        tot = 0.0
+        for _ in range(args.steps):
+            plan.solve(rho, phi)
+            if flush_first:
+                flush.fill_(1)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            plan.source(rho, phi, hyd["omega"], hyd["p"], hyd["s"], hyd["t"], hyd["a"], delt)
+            a1.record(stream)
+            torch.cuda.synchronize()
+            tot += a0.elapsed_time(a1)
+        src[name] = tot / args.steps
+    hbm, kind = peaks()
+    sb = source_bytes_per_launch()
+    achieved = sb / (src["after_l2_flush"] * 1e-3) / 1e9
+    line = {"metric": "gravity steps/s @256x128x256: BDYGEN+POT3, ExternalPot, SOURCE", "value":
+            args.steps / (ms * 1e-3), "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed: f16 hi/lo tensor-core + f32 + f64; f64 star potential and sources"
+            if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": "one time step's gravity: seeded disk, star at (0.0031, 0.7 rad), "
+                                   "random OMEGA, P, S, T, A; device arrays", "precision": args.precision,
+                       "l2": "SOURCE timed after a 256 MiB L2 flush for the roofline"},
+            "gpu_launches": gpu_launches,
+            "inverse_ms": inv, "source_ms": src,
+            "roofline_source": {"bound": "hbm", "achieved": achieved, "peak": hbm,
+                                "unit": "GB/s", "frac": achieved / hbm, "peak_kind": kind,
+                                "algorithmic_bytes": sb},
+            "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- serving workload
 def run_serving_workload(args):
     """Poisson request streams (mean rates --rates) of seeded disks with the
@@ -405,9 +508,10 @@ def main():
     ap.add_argument("--latency-samples", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="pot3", choices=["pot3", "batch", "serving"],
+    ap.add_argument("--workload", default="pot3", choices=["pot3", "batch", "serving", "step"],
                     help="pot3: 256x128x256 mixed (default); batch: 64 uneven grids from one captured "
-                         "graph; serving: Poisson request stream with p50/p99 latency")
+                         "graph; serving: Poisson request stream with p50/p99 latency; step: one time "
+                         "step's gravity (solve, star potential, SOURCE terms)")
     ap.add_argument("--rates", default="200,1000,5000", help="serving: mean arrival rates (req/s)")
     ap.add_argument("--requests", type=int, default=400, help="serving: requests per rate")
     args = ap.parse_args()
@@ -419,6 +523,8 @@ def main():
         return run_batch_workload(args)
     if args.workload == "serving":
         return run_serving_workload(args)
+    if args.workload == "step":
+        return run_step_workload(args)
 
     import torch
     import chymera_uo_b200 as chy

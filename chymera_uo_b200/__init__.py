@@ -43,12 +43,28 @@ class ChyGrid(C.Structure):
 
 class ChyDiag(C.Structure):
     _fields_ = [("tmass", C.c_double), ("phichk", C.c_double), ("klocat", C.c_int),
-                ("iterations", C.c_int), ("corr_rel", C.c_double * 8)]
+                ("iterations", C.c_int), ("corr_rel", C.c_double * 8),
+                ("indirectx", C.c_double), ("indirecty", C.c_double)]
 
     def as_dict(self):
         return {"tmass": self.tmass, "phichk": self.phichk, "klocat": self.klocat,
                 "iterations": self.iterations,
-                "corr_rel": list(self.corr_rel[: max(0, self.iterations)])}
+                "corr_rel": list(self.corr_rel[: max(0, self.iterations)]),
+                "indirectx": self.indirectx, "indirecty": self.indirecty}
+
+
+class ChyExternal(C.Structure):
+    """ExternalPot's inputs (pot/ExternalPot.f:1-80)."""
+    _fields_ = [("mass_star", C.c_double), ("tmassacc", C.c_double),
+                ("rpstar", C.c_double), ("phi_star", C.c_double),
+                ("indirect", C.c_int), ("jmin", C.c_int)]
+
+
+class ChySourceArgs(C.Structure):
+    """SOURCE's arguments (radhydro/source.f:45-81); device pointers."""
+    _fields_ = [("jmax", C.c_int), ("kmax", C.c_int), ("jmin", C.c_int), ("delt", C.c_double),
+                ("rho", C.c_void_p), ("phi", C.c_void_p), ("omega", C.c_void_p), ("p", C.c_void_p),
+                ("s", C.c_void_p), ("t", C.c_void_p), ("a", C.c_void_p)]
 
 
 class ServerOpts(C.Structure):
@@ -130,6 +146,12 @@ def lib():
         L.chy_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
         L.chy_server_get_stats.restype = i
         L.chy_server_destroy.argtypes = [vp]
+        L.chy_plan_set_external.argtypes = [vp, C.POINTER(ChyExternal)]
+        L.chy_plan_set_external.restype = i
+        L.chy_plan_star_potential.argtypes = [vp, vp, i, vp]
+        L.chy_plan_star_potential.restype = i
+        L.chy_source.argtypes = [vp, C.POINTER(ChySourceArgs), vp]
+        L.chy_source.restype = i
         _lib = L
     return _lib
 
@@ -203,6 +225,49 @@ class Plan:
     def set_coef(self, coef_tensor):
         ptr = None if coef_tensor is None else coef_tensor.data_ptr()
         _check(lib().chy_plan_set_coef(self._p, ptr))
+
+    def set_external(self, mass_star: float | None, tmassacc: float = 0.0, rpstar: float = 0.0,
+                     phi_star: float = 0.0, indirect: bool = False, jmin: int = 2):
+        """Adds the star potential of ExternalPot (pot/ExternalPot.f:1-80) to
+        later solves; ``mass_star=None`` removes it."""
+        if mass_star is None:
+            _check(lib().chy_plan_set_external(self._p, None))
+            return
+        e = ChyExternal(mass_star, tmassacc, rpstar, phi_star, int(indirect), jmin)
+        _check(lib().chy_plan_set_external(self._p, C.byref(e)))
+
+    def star_potential(self, out=None, stream=None):
+        """STARPHI(JMAX+2, KMAX+2, LMAX) of the plan's external potential:
+        into a CUDA tensor ``out`` (column-major), else a new numpy array."""
+        if out is not None and _is_cuda_tensor(out):
+            self._validate(out, True)
+            _check(lib().chy_plan_star_potential(self._p, out.data_ptr(), CHY_PTR_DEVICE,
+                                                 self._stream(stream)))
+            return out
+        if out is None:
+            out = np.zeros(self.shape, dtype=np.float64, order="F")
+        self._validate(out, False)
+        _check(lib().chy_plan_star_potential(self._p, out.ctypes.data, CHY_PTR_HOST, stream or 0))
+        return out
+
+    def source(self, rho, phi, omega, p, s, t, a, delt: float, jmin: int = 2, stream=None):
+        """SOURCE's potential, pressure and rotation terms (radhydro/source.f:45-81)
+        on CUDA tensors (column-major): s, t, a updated in place.  omega, p,
+        s, t, a are (JMAX+2, KMAX+2, LMAX) of the hydro grid; rho, phi the
+        plan's grid."""
+        hshape = tuple(omega.shape)
+        for x in (rho, phi):
+            self._validate(x, True)
+        for x in (omega, p, s, t, a):
+            if not _is_cuda_tensor(x) or tuple(x.shape) != hshape or str(x.dtype) != "torch.float64":
+                raise ValueError(f"hydro arrays must be float64 CUDA tensors of one shape {hshape}")
+            if x.stride() != (1, hshape[0], hshape[0] * hshape[1]):
+                raise ValueError("device arrays must be column-major (Fortran) contiguous")
+        if hshape[2] != self.shape[2]:
+            raise ValueError("hydro and potential grids share LMAX")
+        args = ChySourceArgs(hshape[0] - 2, hshape[1] - 2, jmin, delt, rho.data_ptr(), phi.data_ptr(),
+                             omega.data_ptr(), p.data_ptr(), s.data_ptr(), t.data_ptr(), a.data_ptr())
+        _check(lib().chy_source(self._p, C.byref(args), self._stream(stream)))
 
     def set_profiling(self, on: bool):
         _check(lib().chy_plan_set_profiling(self._p, int(on)))

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -54,6 +55,8 @@ struct Packer {
 };
 
 }  // namespace
+
+static int ensure_host_staging(chy_plan *p);
 
 extern "C" {
 
@@ -155,6 +158,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     size_t o_twf = pk.vec(hp.fwd.twc), o_twonf = pk.vec(hp.fwd.onc), o_permf = pk.vec(hp.fwd.perm), o_rtf = pk.vec(hp.fwd.rt);
     size_t o_twi = pk.vec(hp.inv.twc), o_twoni = pk.vec(hp.inv.onc), o_permi = pk.vec(hp.inv.perm), o_rti = pk.vec(hp.inv.rt);
     size_t o_cosm = pk.vec(hp.cosm), o_sinm = pk.vec(hp.sinm), o_fb = pk.vec(hp.fbasis);
+    size_t o_rhf = pk.vec(hp.rhf), o_zhf = pk.vec(hp.zhf), o_r = pk.vec(hp.r);
     size_t o_rs = pk.vec(hp.ring_sorted), o_sring = pk.vec(hp.sring), o_sub = pk.vec(hp.sub_start);
     size_t o_sterm = pk.vec(hp.sterm);
     size_t o_ct = pk.vec(hp.col_term), o_cp = pk.vec(hp.col_part), o_cm_ = pk.vec(hp.col_m), o_cl = pk.vec(hp.col_l);
@@ -194,6 +198,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     }
     t.cosm = (const double *)(D + o_cosm); t.sinm = (const double *)(D + o_sinm);
     t.fbasis = (const double *)(D + o_fb);
+    t.rhf = (const double *)(D + o_rhf); t.zhf = (const double *)(D + o_zhf); t.r = (const double *)(D + o_r);
     t.ring_sorted = (const int *)(D + o_rs); t.sring = (const double *)(D + o_sring);
     t.sterm = (const double *)(D + o_sterm); t.srow = hp.srow;
     t.sub_start = (const int *)(D + o_sub);
@@ -219,7 +224,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     w.ssub = nsub * 2 * hp.ncol;
     w.sscan = (nsub + 1) * 2 * hp.ncol;
     w.sphac = (size_t)hp.K + 2;
-    w.sdiag = 4;
+    w.sdiag = (size_t)kDiagPart + 2 * (size_t)hp.L;
     // every array starts on a 256-byte boundary (16-byte async copies read them)
     auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };
     const size_t per = al(w.sX * max_batch) + al(w.sW * max_batch) + al(w.sC * max_batch) +
@@ -245,7 +250,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     chy_mixed_bind_work(p, q);
     CHY_CUDA(cudaMemset(p->d_work, 0, p->work_bytes));
     p->nvol = (size_t)(hp.J + 2) * (hp.K + 2) * hp.L;
-    CHY_CUDA(cudaMallocHost(&p->h_diag, sizeof(double) * 4 * max_batch));
+    CHY_CUDA(cudaMallocHost(&p->h_diag, sizeof(double) * kDiagPart * max_batch));
     *out = p;
     return CHY_OK;
 }
@@ -289,6 +294,90 @@ int chy_plan_set_refine(chy_plan *p, int corrections)
         if (st != CHY_OK) return fail(st, "FP64 iterate for two or more corrections");
     }
     p->refine = corrections;
+    return CHY_OK;
+}
+
+int chy_plan_set_external(chy_plan *p, const chy_external *e)
+{
+    if (!p) return fail(CHY_ERR_ARG, "null plan");
+    StarDev x{};
+    if (e) {
+        if (e->indirect && e->jmin < 1) return fail(CHY_ERR_ARG, "JMIN must be >= 1");
+        const HostPlan &hp = p->hp;
+        x.on = 1;
+        x.indirect = e->indirect ? 1 : 0;
+        x.jmin = e->jmin;
+        x.mass = e->mass_star + e->tmassacc;
+        x.mass_star = e->mass_star;
+        // INDIRECTX/Y = RPSTAR*COS/SIN(PHI_STAR) (pot/ExternalPot.f:18-19)
+        x.ix = e->rpstar * std::cos(e->phi_star);
+        x.iy = e->rpstar * std::sin(e->phi_star);
+        x.rof3n = hp.g.rof3n;
+        x.zof3n = hp.g.zof3n;
+        x.dtheta = hp.dtheta;
+    }
+    p->star = x;
+    return CHY_OK;
+}
+
+int chy_plan_star_potential(chy_plan *p, double *starphi, int ptr_kind, void *stream)
+{
+    if (!p || !starphi) return fail(CHY_ERR_ARG, "null plan or output");
+    if (!p->star.on) return fail(CHY_ERR_NOT_SETUP, "no external potential set on the plan");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (ptr_kind == CHY_PTR_DEVICE) {
+        CHY_CUDA(launch_star_fill(p->t, p->w, p->star, p->last_slot, starphi, s));
+        p->launches += 1;
+        return CHY_OK;
+    }
+    if (ptr_kind != CHY_PTR_HOST) return fail(CHY_ERR_ARG, "ptr_kind");
+    int st = ensure_host_staging(p);
+    if (st != CHY_OK) return st;
+    // the first staging slot is free: every host-pointer solve call has
+    // finished with it before returning
+    CHY_CUDA(launch_star_fill(p->t, p->w, p->star, p->last_slot, p->stage, s));
+    p->launches += 1;
+    CHY_CUDA(cudaMemcpyAsync(starphi, p->stage, p->nvol * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CHY_CUDA(cudaStreamSynchronize(s));
+    return CHY_OK;
+}
+
+int chy_source(chy_plan *p, const chy_source_args *a, void *stream)
+{
+    if (!p || !a) return fail(CHY_ERR_ARG, "null plan or arguments");
+    if (!a->rho || !a->phi || !a->omega || !a->p || !a->s || !a->t || !a->a)
+        return fail(CHY_ERR_ARG, "null array");
+    const HostPlan &hp = p->hp;
+    if (a->jmax < 1 || a->kmax < 1 || a->jmax > hp.J || a->kmax > hp.K)
+        return fail(CHY_ERR_DIMS, "hydro JMAX/KMAX must be in 1..the plan's JMAX/KMAX");
+    if (a->jmin < 1) return fail(CHY_ERR_ARG, "JMIN must be >= 1");
+    SourceDev q{};
+    q.J2h = a->jmax + 2;
+    q.K2h = a->kmax + 2;
+    q.J2p = hp.J + 2;
+    q.K2p = hp.K + 2;
+    q.L = hp.L;
+    q.Jh = a->jmax;
+    q.Kh = a->kmax;
+    q.j0 = (a->jmin > 2 ? a->jmin : 2) - 1;   // JSTART (radhydro/source.f:33-37)
+    q.delt = a->delt;
+    q.dr = hp.g.rof3n;
+    q.dz = hp.g.zof3n;
+    q.dtheta = hp.dtheta;
+    // reciprocals of power-of-two spacings are exact: multiplying by them
+    // rounds like dividing
+    auto pow2_inv = [](double d) {
+        int e = 0;
+        return std::isfinite(d) && d > 0.0 && std::frexp(d, &e) == 0.5 ? 1.0 / d : 0.0;
+    };
+    q.inv_dr = pow2_inv(q.dr);
+    q.inv_2dr = pow2_inv(2.0 * q.dr);
+    q.inv_dz = pow2_inv(q.dz);
+    q.R = p->t.r;
+    q.rho = a->rho; q.phi = a->phi; q.omega = a->omega; q.p = a->p;
+    q.S = a->s; q.T = a->t; q.A = a->a;
+    CHY_CUDA(launch_source(q, (cudaStream_t)stream));
+    p->launches += 1;
     return CHY_OK;
 }
 
@@ -385,24 +474,35 @@ static int run_batch(chy_plan *p, const BatchPtrs &bp, int nb, cudaStream_t s)
         if (st != CHY_OK) return st;
     }
     CHY_CUDA(mark(4));
-    CHY_CUDA(launch_inverse(t, bp, p->w, nb, s));
+    int ni = 0;
+    if (p->star.on && p->star.indirect) {
+        CHY_CUDA(launch_star_shift(t, bp, p->w, p->star, nb, s));
+        ni = 2;
+    }
+    int nv = 0;
+    CHY_CUDA(launch_inverse(t, bp, p->w, p->star, nb, s, &nv));
     CHY_CUDA(mark(5));
-    p->launches += 1 + 2 + 1 + nl + 2;
+    p->launches += 1 + 2 + 1 + nl + ni + nv;
+    p->last_slot = nb - 1;
     return CHY_OK;
 }
 
 static int fetch_diag(chy_plan *p, chy_diag *diag, int nb, int first, cudaStream_t s)
 {
     if (!diag) return CHY_OK;
-    CHY_CUDA(cudaMemcpyAsync(p->h_diag, p->w.diag, sizeof(double) * 4 * nb, cudaMemcpyDeviceToHost, s));
+    CHY_CUDA(cudaMemcpy2DAsync(p->h_diag, sizeof(double) * kDiagPart, p->w.diag, sizeof(double) * p->w.sdiag,
+                               sizeof(double) * kDiagPart, nb, cudaMemcpyDeviceToHost, s));
     CHY_CUDA(cudaStreamSynchronize(s));
     const int st = chy_mixed_collect(p, nb);
     if (st != CHY_OK) return fail(st, st == CHY_ERR_TIMEOUT ? "mode solve: bounded wait expired" : "mode solve readback");
     for (int i = 0; i < nb; i++) {
         chy_diag &d = diag[first + i];
-        d.tmass = p->h_diag[4 * i + 0];
-        d.phichk = p->h_diag[4 * i + 1];
-        d.klocat = (int)p->h_diag[4 * i + 2];
+        const double *h = p->h_diag + (size_t)kDiagPart * i;
+        d.tmass = h[0];
+        d.phichk = h[1];
+        d.klocat = (int)h[2];
+        d.indirectx = !p->star.on ? 0.0 : p->star.indirect ? h[kDiagStar] : p->star.ix;
+        d.indirecty = !p->star.on ? 0.0 : p->star.indirect ? h[kDiagStar + 1] : p->star.iy;
         chy_mixed_fill_diag(p, i, &d);
     }
     return CHY_OK;
@@ -478,6 +578,10 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
             double *dr = base + (size_t)i * 2 * p->nvol, *df = dr + p->nvol;
             const double *hr = rho[first + i];
             CHY_CUDA(cudaMemcpyAsync(dr, hr, vb, cudaMemcpyHostToDevice, p->s_h2d));
+            // the external potential updates the cells the solve leaves
+            // alone: start them from the caller's values
+            if (p->star.on)
+                CHY_CUDA(copy_phi_rim(df, phi[first + i], hp.J, hp.K, hp.L, cudaMemcpyHostToDevice, p->s_h2d));
             bp.rho[i] = dr;
             bp.phi[i] = df;
         }
@@ -498,8 +602,11 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         }
         CHY_CUDA(cudaEventRecord(p->ev_done[slot], s));
         CHY_CUDA(cudaStreamWaitEvent(p->s_d2h, p->ev_done[slot], 0));
-        for (int i = 0; i < nb; i++)
+        for (int i = 0; i < nb; i++) {
             CHY_CUDA(copy_phi_write_set(phi[first + i], bp.phi[i], hp.J, hp.K, hp.L, p->s_d2h));
+            if (p->star.on)
+                CHY_CUDA(copy_phi_rim(phi[first + i], bp.phi[i], hp.J, hp.K, hp.L, cudaMemcpyDeviceToHost, p->s_d2h));
+        }
         CHY_CUDA(cudaEventRecord(p->ev_out[slot], p->s_d2h));
         used[slot] = true;
     }
@@ -714,6 +821,7 @@ extern "C" int chy_solve_static(chy_plan *p, const double *rho, double *phi, voi
     CHY_CUDA(launch_bdy_sums(t, w, 1, s));
     CHY_CUDA(launch_bdy_synth(t, w, 1, s));
     CHY_CUDA(launch_solve_fp64(t, w, 1, p->num_sms, s));
-    CHY_CUDA(launch_inverse(t, bp, w, 1, s));
+    int nv = 0;
+    CHY_CUDA(launch_inverse(t, bp, w, StarDev{}, 1, s, &nv));   // POT3 alone
     return CHY_OK;
 }

@@ -12,7 +12,9 @@
 //                          sin m psi_l} rho, ring = k*(J-1) + j.
 //   SUB  [nsub][2][ncol]   per sub-chunk sums of the boundary integrands.
 //   SCAN [nsub+1][2][ncol] exclusive prefix (inside) / suffix (outside) sums.
-//   PHAC [K+2]             ZAXPHI deviations; DIAG [4] TMASS, PHICHK, KLOCAT.
+//   PHAC [K+2]             ZAXPHI deviations
+//   DIAG [8 + 2L]          TMASS, PHICHK, KLOCAT, -, INDIRECTX, INDIRECTY, -, -,
+//                          then per-L partial mass moments of the INDIRECT shift.
 #pragma once
 
 #include <cstdint>
@@ -43,6 +45,8 @@ struct DevTables {
     double sf1, pig4, grav, F1, cmmax, ammin, cnmax;
     FftDev fwd, inv;
     const double *cosm, *sinm;      // [10][L]
+    const double *rhf, *zhf;        // RHF(J+2), ZHF(K+2)
+    const double *r;                // R(J+2)
     const double *fbasis;           // [21][L] transforms of {1, cos m psi, sin m psi}
     // kept rings in ascending spherical radius: ring index, and rsph, C1, S1, DV
     const int *ring_sorted;
@@ -73,6 +77,33 @@ struct Work {
     double *coef;                                    // optional /COEFS/ output (solve 0 only)
 };
 
+// ExternalPot (pot/ExternalPot.f:1-80): the star potential added after POT3.
+struct StarDev {
+    int on = 0;          // add STARPHI to PHI
+    int indirect = 0;    // star position shifted by each solve's disk mass moment
+    int jmin = 2;        // first J of that moment (1-based)
+    double mass = 0.0;   // MASS_STAR + TMASSACC
+    double mass_star = 0.0;
+    double ix = 0.0, iy = 0.0;   // RPSTAR cos PHI_STAR, RPSTAR sin PHI_STAR
+    double rof3n = 0.0, zof3n = 0.0, dtheta = 0.0;
+};
+constexpr int kDiagStar = 4;     // DIAG slots of INDIRECTX, INDIRECTY
+constexpr int kDiagPart = 8;     // first DIAG slot of the per-L moments
+
+// SOURCE's potential, pressure and rotation terms (radhydro/source.f:45-81).
+// Hydro arrays (OMEGA, P, S, T, A) are (J2h, K2h, L); RHO and PHI are the
+// potential grid's (J2p, K2p, L).  All pointers are device pointers.
+struct SourceDev {
+    int J2h, K2h, J2p, K2p, L;
+    int Jh, Kh;          // hydro JMAX, KMAX
+    int j0;              // JSTART - 1 (0-based first J of T and A)
+    double delt, dr, dz, dtheta;
+    double inv_dr, inv_2dr, inv_dz;   // 1/DR, 1/(2 DR), 1/DZ when powers of two, else 0
+    const double *R;     // R(POT3JMAX+2)
+    const double *rho, *phi, *omega, *p;
+    double *S, *T, *A;
+};
+
 // Raises a kernel's dynamic shared-memory limit on the current device the
 // first time a launch needs it; the attribute persists, so later launches make
 // no runtime call (a per-launch cudaFuncSetAttribute stalls the issue stream).
@@ -83,6 +114,17 @@ cudaError_t launch_forward(const DevTables &t, const BatchPtrs &bp, const Work &
 cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStream_t s);
 cudaError_t launch_bdy_synth(const DevTables &t, const Work &w, int nb, cudaStream_t s);
 cudaError_t launch_solve_fp64(const DevTables &t, const Work &w, int nb, int num_sms, cudaStream_t s);
-cudaError_t launch_inverse(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s);
+// Inverse transform into PHI (plus STARPHI when x.on) and the diagnostics;
+// with x.on also the cells POT3 leaves alone; reports its launch count.
+cudaError_t launch_inverse(const DevTables &t, const BatchPtrs &bp, const Work &w, const StarDev &x, int nb,
+                           cudaStream_t s, int *launches);
+// INDIRECT star position of each solve into DIAG (x.on && x.indirect).
+cudaError_t launch_star_shift(const DevTables &t, const BatchPtrs &bp, const Work &w, const StarDev &x, int nb,
+                              cudaStream_t s);
+// SOURCE's first loop nest on device arrays (k_source.cu).
+cudaError_t launch_source(const SourceDev &a, cudaStream_t s);
+// STARPHI(J+2, K+2, L) into out (star position of batch slot `slot` if indirect).
+cudaError_t launch_star_fill(const DevTables &t, const Work &w, const StarDev &x, int slot, double *out,
+                             cudaStream_t s);
 
 }  // namespace chy

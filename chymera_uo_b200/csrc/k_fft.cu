@@ -457,8 +457,36 @@ __global__ void k_coef(DevTables t, Work w)
 // ghosts (pot/pot3.f:289-292) and the ZAXPHI row PHI(JMAX+2, K, :)
 // (pot/pot3.f:350-387); CTAs at K = 2 write the midplane ghosts
 // (pot/pot3.f:293-296).
+// STARPHI of the cell (j, k, l) of PHI(J+2, K+2, L), 0-based, with the star at
+// (ix, iy): the reference's expression in its order of operations, every
+// product and sum rounded on its own (pot/ExternalPot.f:44-49).  COS/SIN of
+// (L-1/2)*DTHETA are the m = 1 rows of COSM/SINM, the same numbers.
+__device__ __forceinline__ double star_phi(const DevTables &t, const StarDev &x, double ix, double iy, int j, int k,
+                                           int l)
+{
+    const double r = t.rhf[j], z = t.zhf[k], c = t.cosm[l], s = t.sinm[l];
+    double q = __dadd_rn(__dmul_rn(r, r), __dmul_rn(z, z));
+    q = __dadd_rn(q, __dmul_rn(ix, ix));
+    q = __dadd_rn(q, __dmul_rn(iy, iy));
+    q = __dsub_rn(q, __dmul_rn(__dmul_rn(2.0, r), __dadd_rn(__dmul_rn(c, ix), __dmul_rn(s, iy))));
+    return __ddiv_rn(-x.mass, __dsqrt_rn(q));
+}
+
+// Star position of solve b: fixed, or the solve's INDIRECT shift.
+__device__ __forceinline__ void star_pos(const StarDev &x, const Work &w, int b, double *ix, double *iy)
+{
+    if (x.indirect) {
+        const double *d = w.diag + (size_t)b * w.sdiag;
+        *ix = d[kDiagStar];
+        *iy = d[kDiagStar + 1];
+    } else {
+        *ix = x.ix;
+        *iy = x.iy;
+    }
+}
+
 template <int L>
-__global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work w)
+__global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work w, StarDev x)
 {
     using T = Tile<L>;
     constexpr int n = T::N;
@@ -490,19 +518,26 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
         const int src = fs.perm[l >> 1];
         return 0.5 * A[(2 * src + (l & 1)) * T::RS + c];
     };
+    // PHI = PHI + STARPHI after POT3 (pot/ExternalPot.f:50), fused into the
+    // stores: v is POT3's value of the cell (jj, kk, l)
+    double ix = 0.0, iy = 0.0;
+    if (x.on) star_pos(x, w, b, &ix, &iy);
+    auto out = [&](int jj, int kk, int l, double v) -> double {
+        return x.on ? __dadd_rn(v, star_phi(t, x, ix, iy, jj, kk, l)) : v;
+    };
     for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
         const int c = i % T::TC, l = i / T::TC, j = j0 + c;
         if (j < t.J) {
             const double v = sample(l, c);
-            phi[(size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] = v;
-            if (k == 0) phi[(size_t)(j + 1) + (size_t)J2 * ((size_t)K2 * l)] = v;   // PHI(J,1,L)
+            phi[(size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] = out(j + 1, k + 1, l, v);
+            if (k == 0) phi[(size_t)(j + 1) + (size_t)J2 * ((size_t)K2 * l)] = out(j + 1, 0, l, v);   // PHI(J,1,L)
         }
     }
     if (j0 == 0) {
         for (int l = threadIdx.x; l < L; l += blockDim.x) {
-            const double v = sample((l + n) % L, 0);                 // PHI(2,K,L+-N)
-            phi[(size_t)J2 * ((k + 1) + (size_t)K2 * l)] = v;       // PHI(1,K,L)
-            if (k == 0) phi[(size_t)J2 * ((size_t)K2 * l)] = v;     // PHI(1,1,L)
+            const double v = sample((l + n) % L, 0);                             // PHI(2,K,L+-N)
+            phi[(size_t)J2 * ((k + 1) + (size_t)K2 * l)] = out(0, k + 1, l, v);   // PHI(1,K,L)
+            if (k == 0) phi[(size_t)J2 * ((size_t)K2 * l)] = out(0, 0, l, v);     // PHI(1,1,L)
         }
         // ZAXPHI: Neville extrapolation to r = 0 across +-RHF (pot/pot3.f:354-378)
         const int lm = L / 2, np = t.npoint;
@@ -524,8 +559,8 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
             }
             const double ph = p2[np];
             red[l] = ph;
-            phi[(size_t)(t.J + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] = ph;
-            phi[(size_t)(t.J + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * (l + lm))] = ph;
+            phi[(size_t)(t.J + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] = out(t.J + 1, k + 1, l, ph);
+            phi[(size_t)(t.J + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * (l + lm))] = out(t.J + 1, k + 1, l + lm, ph);
         }
         __syncthreads();
         // PHAC(K): the first largest-|ER| deviation, ER = 1 - PH(L)/PHMAX,
@@ -554,6 +589,99 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
             if (threadIdx.x == 0) w.phac[(size_t)b * w.sphac + (k + 2)] = em;
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// ExternalPot's other cells, its INDIRECT star position and STARPHI itself
+// ---------------------------------------------------------------------------
+// PHI = PHI + STARPHI on the cells POT3 does not write: PHI(:, KMAX+2, L) and
+// PHI(JMAX+2, 1, L) (pot/ExternalPot.f:42-50 covers the whole grid).
+// Grid (L, batch).
+__global__ void __launch_bounds__(128) k_star_rim(DevTables t, BatchPtrs bp, Work w, StarDev x)
+{
+    const int l = blockIdx.x, b = blockIdx.y, J2 = t.J + 2, K2 = t.K + 2;
+    double *phi = bp.phi[b];
+    double ix, iy;
+    star_pos(x, w, b, &ix, &iy);
+    for (int j = threadIdx.x; j <= J2; j += blockDim.x) {
+        // j < J2: row K = KMAX+2; j == J2: the cell (JMAX+2, 1)
+        const int jj = j < J2 ? j : t.J + 1, kk = j < J2 ? t.K + 1 : 0;
+        const size_t at = (size_t)jj + (size_t)J2 * ((size_t)kk + (size_t)K2 * l);
+        phi[at] = __dadd_rn(phi[at], star_phi(t, x, ix, iy, jj, kk, l));
+    }
+}
+
+// INDIRECT (pot/ExternalPot.f:21-34): the disk's mass moment of plane L,
+//   sum over K = 2..KMAX1, J = JMIN..JMAX1 of THISMASS*COS(PSI_L)*RHF(J)
+//   (and SIN), THISMASS = RHO*RHF(J)*ROF3N*ZOF3N*2*DTHETA,
+// into DIAG[kDiagPart + 2L..].  Grid (L, batch); fixed summation order.
+__global__ void __launch_bounds__(256) k_star_moment(DevTables t, BatchPtrs bp, Work w, StarDev x)
+{
+    const int l = blockIdx.x, b = blockIdx.y, J2 = t.J + 2, K2 = t.K + 2;
+    const double *rho = bp.rho[b] + (size_t)J2 * K2 * l;
+    const int j0 = x.jmin - 1, nj = t.J + 1 - j0;   // 0-based J = JMIN-1 .. JMAX
+    const double c = t.cosm[l], s = t.sinm[l];
+    double sx = 0.0, sy = 0.0;
+    if (nj > 0) {
+        for (int i = threadIdx.x; i < nj * t.K; i += blockDim.x) {
+            const int j = j0 + i % nj, k = 1 + i / nj;
+            const double r = t.rhf[j];
+            double m = __dmul_rn(rho[(size_t)j + (size_t)J2 * k], r);
+            m = __dmul_rn(m, x.rof3n);
+            m = __dmul_rn(m, x.zof3n);
+            m = __dmul_rn(m, 2.0);
+            m = __dmul_rn(m, x.dtheta);
+            sx = __dadd_rn(sx, __dmul_rn(__dmul_rn(m, c), r));
+            sy = __dadd_rn(sy, __dmul_rn(__dmul_rn(m, s), r));
+        }
+    }
+    __shared__ double part[2][8];
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    const int wp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { part[0][wp] = sx; part[1][wp] = sy; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ax = 0.0, ay = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) { ax += part[0][i]; ay += part[1][i]; }
+        double *d = w.diag + (size_t)b * w.sdiag + kDiagPart + 2 * l;
+        d[0] = ax;
+        d[1] = ay;
+    }
+}
+
+// INDIRECTX/Y = -(RPSTAR*COS/SIN(PHI_STAR) + moment)/MASS_STAR
+// (pot/ExternalPot.f:18-19,35-36).  One warp per solve.
+__global__ void k_star_shift(DevTables t, Work w, StarDev x)
+{
+    const int b = blockIdx.x;
+    double *d = w.diag + (size_t)b * w.sdiag;
+    double sx = 0.0, sy = 0.0;
+    for (int l = threadIdx.x; l < t.L; l += 32) {
+        sx += d[kDiagPart + 2 * l];
+        sy += d[kDiagPart + 2 * l + 1];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    if (threadIdx.x == 0) {
+        d[kDiagStar] = -(x.ix + sx) / x.mass_star;
+        d[kDiagStar + 1] = -(x.iy + sy) / x.mass_star;
+    }
+}
+
+// STARPHI(J+2, K+2, L) (/GAP/) for the star position of batch slot `slot`.
+// Grid (K+2, L).
+__global__ void __launch_bounds__(128) k_star_fill(DevTables t, Work w, StarDev x, int slot, double *out)
+{
+    const int k = blockIdx.x, l = blockIdx.y, J2 = t.J + 2, K2 = t.K + 2;
+    double ix, iy;
+    star_pos(x, w, slot, &ix, &iy);
+    for (int j = threadIdx.x; j < J2; j += blockDim.x)
+        out[(size_t)j + (size_t)J2 * ((size_t)k + (size_t)K2 * l)] = star_phi(t, x, ix, iy, j, k, l);
 }
 
 // PHICHK / KLOCAT (pot/pot3.f:391-399) and TMASS (pot/boundary.f:554).
@@ -593,17 +721,21 @@ static cudaError_t forward_l(const DevTables &t, const BatchPtrs &bp, const Work
 }
 
 template <int L>
-static cudaError_t inverse_l(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s);
-
-template <int L>
-static cudaError_t inverse_l(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s)
+static cudaError_t inverse_l(const DevTables &t, const BatchPtrs &bp, const Work &w, const StarDev &x, int nb,
+                             cudaStream_t s, int *launches)
 {
     using T = Tile<L>;
     const size_t sm = tile_bytes<L>() + (size_t)(L / 2) * 8 + fft_table_bytes<L>();
     cudaError_t e = ensure_smem((const void *)k_inverse<L>, sm);
     if (e != cudaSuccess) return e;
-    k_inverse<L><<<dim3((t.J + T::TC - 1) / T::TC, t.K, nb), 256, sm, s>>>(t, bp, w);
+    k_inverse<L><<<dim3((t.J + T::TC - 1) / T::TC, t.K, nb), 256, sm, s>>>(t, bp, w, x);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    *launches = 2;
+    if (x.on) {
+        k_star_rim<<<dim3(L, nb), 128, 0, s>>>(t, bp, w, x);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        *launches = 3;
+    }
     k_diag<<<nb, 32, 0, s>>>(t, w);
     return cudaGetLastError();
 }
@@ -633,9 +765,27 @@ cudaError_t launch_bdy_synth(const DevTables &t, const Work &w, int nb, cudaStre
     return cudaGetLastError();
 }
 
-cudaError_t launch_inverse(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s)
+cudaError_t launch_inverse(const DevTables &t, const BatchPtrs &bp, const Work &w, const StarDev &x, int nb,
+                           cudaStream_t s, int *launches)
 {
-    CHY_DISPATCH_L(inverse_l, t, bp, w, nb, s)
+    CHY_DISPATCH_L(inverse_l, t, bp, w, x, nb, s, launches)
+}
+
+cudaError_t launch_star_shift(const DevTables &t, const BatchPtrs &bp, const Work &w, const StarDev &x, int nb,
+                              cudaStream_t s)
+{
+    k_star_moment<<<dim3(t.L, nb), 256, 0, s>>>(t, bp, w, x);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_star_shift<<<nb, 32, 0, s>>>(t, w, x);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_star_fill(const DevTables &t, const Work &w, const StarDev &x, int slot, double *out,
+                             cudaStream_t s)
+{
+    k_star_fill<<<dim3(t.K + 2, t.L), 128, 0, s>>>(t, w, x, slot, out);
+    return cudaGetLastError();
 }
 
 // Compile-time stage structure used by the kernels, for the plan to compare

@@ -41,6 +41,8 @@ struct chy_plan {
     double *coef_host = nullptr;   // /COEFS/ host destination (chy_plan_set_coef_host)
     double *coef_dev = nullptr;    // device COEF buffer owned by the plan
     size_t coef_bytes = 0;
+    chy::StarDev star;             // ExternalPot (chy_plan_set_external)
+    int last_slot = 0;             // batch slot of the latest solve launched
     bool profile = false;
     // One event set per profiled launch sequence, read back lazily (after
     // the caller has synchronised) so profiling adds no host waits.
@@ -63,6 +65,19 @@ inline cudaError_t copy_phi_write_set(double *host, const double *dev, int J, in
                                       cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return e;
     return cudaMemcpy2DAsync(host, plane, dev, plane, ((size_t)J + 1) * sizeof(double), L, cudaMemcpyDeviceToHost, s);
+}
+
+// Copies the cells of PHI that a solve never writes, PHI(:, KMAX+2, :) and
+// PHI(JMAX+2, 1, :), between the caller's host array and a device copy (in
+// either direction, by `kind`).  The external potential updates them in place.
+inline cudaError_t copy_phi_rim(double *dst, const double *src, int J, int K, int L, cudaMemcpyKind kind,
+                                cudaStream_t s)
+{
+    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2, plane = J2 * K2 * sizeof(double);
+    const size_t top = J2 * ((size_t)K + 1);
+    cudaError_t e = cudaMemcpy2DAsync(dst + top, plane, src + top, plane, J2 * sizeof(double), L, kind, s);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy2DAsync(dst + J + 1, plane, src + J + 1, plane, sizeof(double), L, kind, s);
 }
 
 // One launch sequence over nb device-pointer solves (api.cu).

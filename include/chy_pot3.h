@@ -74,6 +74,8 @@ typedef struct chy_diag {
     int iterations;            /* approximate solves performed (mixed: 1 +      */
                                /* corrections; 0 for the FP64 path)             */
     double corr_rel[8];        /* ||delta_i|| / ||x_{i+1}|| of solve i           */
+    double indirectx, indirecty; /* star position the external potential used  */
+                               /* (/POIS/ INDIRECTX/Y); 0 without one           */
 } chy_diag;
 
 typedef struct chy_plan chy_plan;
@@ -164,6 +166,63 @@ int chy_plan_set_coef_host(chy_plan *p, double *coef_host);
  * more keep an FP64 iterate in device memory, allocated by this call (one
  * more grid volume per batch slot). */
 int chy_plan_set_refine(chy_plan *p, int corrections);
+
+/* ---- ExternalPot (pot/ExternalPot.f:1-80) --------------------------------
+ * The central star's potential, added to PHI right after POT3 as the
+ * EXTERNAL_POT build does every time step (radhydro/3dhyd-main.f:510-512):
+ *   STARPHI(J,K,L) = -(MASS_STAR+TMASSACC) / SQRT(RHF(J)**2 + ZHF(K)**2
+ *       + IX**2 + IY**2 - 2 RHF(J) (COS(PSI_L) IX + SIN(PSI_L) IY)),
+ *   PSI_L = (L-1/2) DTHETA, PHI = PHI + STARPHI on every cell of the grid.
+ * IX, IY = RPSTAR*COS(PHI_STAR), RPSTAR*SIN(PHI_STAR) (ExternalPot.f:18-19);
+ * with `indirect` set (INDIRECT builds, ExternalPot.f:21-40) each solve adds
+ * its disk's mass moment over J = JMIN..JMAX+1, K = 2..KMAX+1 and divides by
+ * -MASS_STAR.  The add is fused into the inverse transform's stores; the
+ * cells POT3 does not write (K = KMAX+2, and J = JMAX+2 at K = 1) are updated
+ * in place, so for host-pointer solves those cells of the caller's PHI are
+ * read in as well as written back. */
+typedef struct chy_external {
+    double mass_star, tmassacc;  /* MASS_STAR, TMASSACC (/GAP/, globals.h:28)    */
+    double rpstar, phi_star;     /* star position (/movingstar/, globals.h:5-6)  */
+    int indirect;                /* 1: INDIRECT build's centre-of-mass shift     */
+    int jmin;                    /* JMIN of that shift (hydroparam.h:23: 2)      */
+} chy_external;
+/* Sets (ext non-NULL) or clears (NULL) the external potential of the plan's
+ * later solves through chy_solve / chy_solve_batch / chy_solve_multi.
+ * chy_solve_static and the server solve POT3 alone. */
+int chy_plan_set_external(chy_plan *p, const chy_external *ext);
+/* Writes STARPHI(JMAX+2, KMAX+2, LMAX) (/GAP/ STARPHI) for the plan's
+ * external potential: with `indirect`, for the star position of the plan's
+ * latest solve (the last one of its most recent solve call), as the
+ * reference's array holds it after the time step's solve.  Call it on the
+ * stream of that solve, or after it.  starphi is a device or host pointer per
+ * ptr_kind; host-pointer calls synchronise `stream`. */
+int chy_plan_star_potential(chy_plan *p, double *starphi, int ptr_kind, void *stream);
+
+/* ---- SOURCE's potential, pressure and rotation terms ----------------------
+ * The first loop nest of SOURCE (radhydro/source.f:45-81, BINARY = 0), the
+ * consumer of the PHI a solve writes, on device arrays in the reference's
+ * layouts, with the plan's R, ROF3N (DR), ZOF3N (DZ) and DTHETA.  For
+ * L = 1..LMAX (periodic in L), K = 2..KMAX+1 of the hydro grid:
+ *   S += DELT*(R(J)(RHO_J+RHO_J-1)(OMEGA_J+OMEGA_J-1)**2/8
+ *              - (RHO_J+RHO_J-1)(PHI_J-PHI_J-1)/(2 DR) - (P_J-P_J-1)/DR),
+ *        J = JSTART+1..JMAX+1;
+ *   T -= DELT*((RHO_K+RHO_K-1)/2 (PHI_K-PHI_K-1)/DZ + (P_K-P_K-1)/DZ),
+ *   A -= DELT*(RHO (PHI_L+1-PHI_L-1) + P_L+1 - P_L-1)/(2 DTHETA),
+ *        J = JSTART..JMAX+1;  JSTART = MAX(JMIN, 2).
+ * Each operation rounds as the reference's does: bit-identical results.
+ * Issued on `stream` after a solve on the same stream, it finds most of PHI
+ * still in L2. */
+typedef struct chy_source_args {
+    int jmax, kmax;            /* hydro JMAX, KMAX (<= the plan's; hydroparam.h:16-17) */
+    int jmin;                  /* JMIN (hydroparam.h:23)                             */
+    double delt;               /* DELT                                               */
+    const double *rho, *phi;   /* RHO, PHI(POT3JMAX+2, POT3KMAX+2, LMAX) (/POIS/)    */
+    const double *omega, *p;   /* OMEGA, P(JMAX+2, KMAX+2, LMAX)                     */
+    double *s, *t, *a;         /* S, T, A(JMAX+2, KMAX+2, LMAX), updated in place     */
+} chy_source_args;
+/* Device pointers only; S, T, A must not overlap the input arrays.
+ * Asynchronous on `stream`. */
+int chy_source(chy_plan *p, const chy_source_args *args, void *stream);
 
 /* Bytes of device work space the plan holds (tables + per-solve scratch). */
 long long chy_plan_device_bytes(const chy_plan *p);

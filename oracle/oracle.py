@@ -54,6 +54,8 @@ def lib():
         L.ora_blktri_state_size.restype = i
         L.ora_blktri.argtypes = [vp, i, i, i, dp, dp, dp, i, i, dp, dp, dp, i, dp, ip, dp]
         L.ora_blktri_wsize.restype = i
+        L.ora_external_pot.argtypes = [vp, d, d, d, d, i, i, dp, dp]
+        L.ora_source.argtypes = [i, i, i, i, i, i, d, d, d, d, dp, dp, dp, dp, dp, dp, dp, dp]
         L.ora_blktri_wsize.argtypes = [i, i]
         _lib = L
     return _lib
@@ -170,6 +172,16 @@ class Oracle:
         lib().ora_inside(self._c, _dp(out))
         return {"tmass": out[0], "phichk": out[1], "klocat": int(out[2])}
 
+    def external_pot(self, mass_star: float, tmassacc: float = 0.0, rpstar: float = 0.0,
+                     phi_star: float = 0.0, indirect: bool = False, jmin: int = 2):
+        """ExternalPot (pot/ExternalPot.f:1-80) on the context's PHI: adds
+        STARPHI in place.  Returns (STARPHI, (INDIRECTX, INDIRECTY))."""
+        sp = np.zeros((self.J + 2, self.K + 2, self.L), order="F")
+        ixy = np.zeros(2)
+        lib().ora_external_pot(self._c, mass_star, tmassacc, rpstar, phi_star, int(indirect), jmin,
+                               _dp(sp), _dp(ixy))
+        return sp, (float(ixy[0]), float(ixy[1]))
+
     def solve(self, rho: np.ndarray, delr: float | None = None, delz: float | None = None,
               isym: int = 2, maxtrm: int = 10, redge: float = 0.0, npoint: int = 8,
               phi_init: np.ndarray | None = None) -> np.ndarray:
@@ -191,6 +203,21 @@ class Oracle:
             raise RuntimeError("BDYGEN called before SETBDY")
         self.pot3(npoint, 0)
         return np.array(self.phi, order="F", copy=True)
+
+
+def source(r, rho, phi, omega, p, s, t, a, delt, dr, dz, dtheta, jmin=2):
+    """SOURCE's first loop nest (radhydro/source.f:45-81) on Fortran-ordered
+    arrays: omega, p, s, t, a of the hydro grid (JMAX+2, KMAX+2, LMAX); rho,
+    phi of the potential grid.  s, t, a are updated in place."""
+    j2, k2, lmax = omega.shape
+    j2p, k2p, _ = rho.shape
+    for x in (rho, phi, omega, p, s, t, a):
+        assert x.dtype == np.float64 and x.flags.f_contiguous
+    for x in (omega, p, s, t, a):
+        assert x.shape == (j2, k2, lmax)
+    assert phi.shape == rho.shape and r.shape[0] >= j2p
+    lib().ora_source(j2 - 2, k2 - 2, lmax, j2p, k2p, jmin, delt, dr, dz, dtheta, _dp(np.ascontiguousarray(r)),
+                     _dp(rho), _dp(phi), _dp(omega), _dp(p), _dp(s), _dp(t), _dp(a))
 
 
 def blktri_solve(an, bn, cn, am, bm, cm, y):

@@ -2097,3 +2097,91 @@ void ora_pot3(ora_ctx *c, int npoint, int iprint)
     free(DENOMR + 1); free(RD2 + 1); free(RD3 + 1); free(DENOMZ + 1); free(ZD2 + 1);
     free(XLAMM + 1);
 }
+
+/* ------------------------------------------------------------------------ */
+/* ExternalPot (pot/ExternalPot.f:1-80): the central star's potential added  */
+/* to PHI after POT3 (radhydro/3dhyd-main.f:510-512, EXTERNAL_POT builds).   */
+/* ------------------------------------------------------------------------ */
+/* INDIRECTX/Y start at RPSTAR*COS/SIN(PHI_STAR) (ExternalPot.f:18-19).  With
+ * indirect != 0 (INDIRECT builds, ExternalPot.f:21-40) the disk's mass
+ * moment over L, K = 2..KMAX1, J = JMIN..JMAX1 is summed in the reference's
+ * serial loop order, added as an OpenMP reduction adds it to the start value,
+ * and divided by -MASS_STAR.  STARPHI over the whole grid (ExternalPot.f:42-54)
+ * is added to PHI and, if starphi is not NULL, stored there.  ixy (if not
+ * NULL) receives INDIRECTX, INDIRECTY. */
+void ora_external_pot(ora_ctx *c, double mass_star, double tmassacc, double rpstar, double phi_star,
+                      int indirect, int jmin, double *starphi, double *ixy)
+{
+    const int jmax = c->jmax, kmax = c->kmax, lmax = c->lmax;
+    const double dtheta = c->dtheta, half = 0.5, two = 2.0;
+    double ix = rpstar * cos(phi_star), iy = rpstar * sin(phi_star);
+    if (indirect) {
+        double sx = 0.0, sy = 0.0;
+        for (int l = 1; l <= lmax; l++)
+            for (int k = 2; k <= kmax + 1; k++)
+                for (int j = jmin; j <= jmax + 1; j++) {
+                    const double rhf = c->rhf[j - 1];
+                    const double m = RHO_(c, j, k, l) * rhf * c->rof3n * c->zof3n * two * dtheta;
+                    sx = sx + m * cos(((double)(l - 1) + half) * dtheta) * rhf;
+                    sy = sy + m * sin(((double)(l - 1) + half) * dtheta) * rhf;
+                }
+        ix = -(ix + sx) / mass_star;
+        iy = -(iy + sy) / mass_star;
+    }
+    const double mass = mass_star + tmassacc;
+    for (int l = 1; l <= lmax; l++) {
+        const double cl = cos(((double)(l - 1) + half) * dtheta), sl = sin(((double)(l - 1) + half) * dtheta);
+        for (int k = 1; k <= kmax + 2; k++)
+            for (int j = 1; j <= jmax + 2; j++) {
+                const double rhf = c->rhf[j - 1], zhf = c->zhf[k - 1];
+                const double sp = -mass / sqrt(rhf * rhf + zhf * zhf + ix * ix + iy * iy -
+                                               two * rhf * (cl * ix + sl * iy));
+                PHI_(c, j, k, l) = PHI_(c, j, k, l) + sp;
+                if (starphi)
+                    starphi[((size_t)j - 1) + (size_t)(jmax + 2) * (((size_t)k - 1) + (size_t)(kmax + 2) * ((size_t)l - 1))] = sp;
+            }
+    }
+    if (ixy) { ixy[0] = ix; ixy[1] = iy; }
+}
+
+/* ------------------------------------------------------------------------ */
+/* SOURCE's first loop nest (radhydro/source.f:45-81, BINARY = 0): the       */
+/* potential, pressure and rotation terms of the S, T, A momenta.            */
+/* ------------------------------------------------------------------------ */
+/* Hydro arrays omega, p, s, t, a are (jmax+2, kmax+2, lmax); rho and phi are
+ * the potential grid's (j2p, k2p, lmax); r is R(j2p).  Column-major. */
+void ora_source(int jmax, int kmax, int lmax, int j2p, int k2p, int jmin, double delt, double dr, double dz,
+                double dtheta, const double *r, const double *rho, const double *phi, const double *omega,
+                const double *p, double *s, double *t, double *a)
+{
+    const double quarter = 0.25, half = 0.5, two = 2.0;
+    const size_t j2 = (size_t)jmax + 2, k2 = (size_t)kmax + 2;
+#define H_(x, j, k, l) (x)[((size_t)(j) - 1) + j2 * (((size_t)(k) - 1) + k2 * ((size_t)(l) - 1))]
+#define P_(x, j, k, l) (x)[((size_t)(j) - 1) + (size_t)j2p * (((size_t)(k) - 1) + (size_t)k2p * ((size_t)(l) - 1))]
+    const int jstart = jmin > 2 ? jmin : 2;   /* radhydro/source.f:33-37 */
+    for (int l = 1; l <= lmax; l++) {
+        int lm = l - 1, lp = l + 1;
+        if (l == 1) lm = lmax;
+        if (l == lmax) lp = 1;
+        for (int k = 2; k <= kmax + 1; k++) {
+            for (int j = jstart + 1; j <= jmax + 1; j++) {
+                const double om = H_(omega, j, k, l) + H_(omega, j - 1, k, l);
+                H_(s, j, k, l) = H_(s, j, k, l) +
+                    delt * (r[j - 1] * (P_(rho, j, k, l) + P_(rho, j - 1, k, l)) * (om * om) * quarter * half -
+                            (P_(rho, j, k, l) + P_(rho, j - 1, k, l)) * (P_(phi, j, k, l) - P_(phi, j - 1, k, l)) /
+                                (two * dr) -
+                            (H_(p, j, k, l) - H_(p, j - 1, k, l)) / dr);
+            }
+            for (int j = jstart; j <= jmax + 1; j++)
+                H_(t, j, k, l) = H_(t, j, k, l) -
+                    delt * (half * (P_(rho, j, k, l) + P_(rho, j, k - 1, l)) * (P_(phi, j, k, l) - P_(phi, j, k - 1, l)) / dz +
+                            (H_(p, j, k, l) - H_(p, j, k - 1, l)) / dz);
+            for (int j = jstart; j <= jmax + 1; j++)
+                H_(a, j, k, l) = H_(a, j, k, l) -
+                    delt * (P_(rho, j, k, l) * (P_(phi, j, k, lp) - P_(phi, j, k, lm)) + H_(p, j, k, lp) - H_(p, j, k, lm)) /
+                        (two * dtheta);
+        }
+    }
+#undef H_
+#undef P_
+}

@@ -63,6 +63,22 @@ void ora_inside(ora_ctx *c, double *out3);
 /* PHAC(K), K=1..KMAX2, from the last ZAXPHI */
 double *ora_phac(ora_ctx *c);
 
+/* ExternalPot (pot/ExternalPot.f:1-80) on the context's PHI after POT3:
+ * adds STARPHI = -(MASS_STAR+TMASSACC)/|x - x_star| everywhere (starphi, if
+ * not NULL, receives it) with the star at INDIRECTX/Y = RPSTAR*COS/SIN(PHI_STAR),
+ * or, indirect != 0 (INDIRECT builds), shifted by the disk's mass moment over
+ * J = JMIN..JMAX1 (ExternalPot.f:21-40).  ixy (if not NULL) gets INDIRECTX/Y. */
+void ora_external_pot(ora_ctx *c, double mass_star, double tmassacc, double rpstar, double phi_star,
+                      int indirect, int jmin, double *starphi, double *ixy);
+
+/* SOURCE's potential, pressure and rotation terms (radhydro/source.f:45-81,
+ * BINARY = 0) for a hydro grid jmax x kmax x lmax: omega, p, s, t, a are
+ * (jmax+2, kmax+2, lmax); rho, phi are (j2p, k2p, lmax); r is R(j2p).  s, t, a
+ * are updated in place. */
+void ora_source(int jmax, int kmax, int lmax, int j2p, int k2p, int jmin, double delt, double dr, double dz,
+                double dtheta, const double *r, const double *rho, const double *phi, const double *omega,
+                const double *p, double *s, double *t, double *a);
+
 /* Low-level routines, exported for unit tests. Arrays are 0-based views of the
  * Fortran 1-based arrays. */
 void ora_fft(double *a, double *b, int ntot, int n, int nspan, int isn, int literal_r8);

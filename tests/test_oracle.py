@@ -289,3 +289,107 @@ def test_oracle_threads_agree_with_serial(ora):
     p1 = ora.Oracle(64, 32, 64, nthreads=1).solve(rho)
     p4 = ora.Oracle(64, 32, 64, nthreads=4).solve(rho)
     assert np.linalg.norm(p4 - p1) / np.linalg.norm(p1) < 1e-13
+
+
+# ---------------------------------------------------------------------------
+# ExternalPot (pot/ExternalPot.f:1-80)
+# ---------------------------------------------------------------------------
+def _starphi_scalar(rhf, zhf, L, dtheta, mass, ix, iy):
+    """pot/ExternalPot.f:44-49 term by term with Python floats (libm cos/sin)."""
+    import math
+    out = np.zeros((len(rhf), len(zhf), L), order="F")
+    for l in range(1, L + 1):
+        c = math.cos((float(l - 1) + 0.5) * dtheta)
+        s = math.sin((float(l - 1) + 0.5) * dtheta)
+        for k, z in enumerate(zhf):
+            for j, r in enumerate(rhf):
+                out[j, k, l - 1] = -mass / math.sqrt(r * r + z * z + ix * ix + iy * iy - 2.0 * r * (c * ix + s * iy))
+    return out
+
+
+def test_external_pot_centred_star_is_point_mass(ora):
+    J, K, L = 16, 8, 16
+    o = ora.Oracle(J, K, L)
+    o.set_grid(1.0 / J, 0.5 / K)
+    before = np.array(o.phi)
+    sp, (ix, iy) = o.external_pot(mass_star=1.0, tmassacc=0.25)
+    assert ix == 0.0 and iy == 0.0
+    R, Z = np.meshgrid(o.rhf, o.zhf, indexing="ij")
+    want = -1.25 / np.sqrt(R * R + Z * Z)
+    assert np.array_equal(sp, np.repeat(want[:, :, None], L, axis=2))
+    assert np.array_equal(o.phi, before + sp)
+
+
+def test_external_pot_offset_star_term_by_term(ora):
+    import math
+    J, K, L = 8, 4, 8
+    o = ora.Oracle(J, K, L)
+    o.set_grid(1.0 / J, 0.5 / K)
+    rng = np.random.default_rng(3)
+    o.phi[...] = rng.standard_normal(o.phi.shape)
+    before = np.array(o.phi)
+    sp, (ix, iy) = o.external_pot(mass_star=0.9, tmassacc=0.01, rpstar=0.013, phi_star=2.1)
+    assert ix == 0.013 * math.cos(2.1) and iy == 0.013 * math.sin(2.1)
+    want = _starphi_scalar(o.rhf, o.zhf, L, 2.0 * 3.1415926535897932 / L, 0.9 + 0.01, ix, iy)
+    assert np.array_equal(sp, want)
+    assert np.array_equal(o.phi, before + sp)
+    # the potential is lowest at the cell nearest the star
+    assert np.isfinite(sp).all() and (sp < 0).all()
+
+
+def test_external_pot_indirect_shift(ora):
+    import math
+    J, K, L = 16, 8, 16
+    o = ora.Oracle(J, K, L)
+    o.set_grid(1.0 / J, 0.5 / K)
+    rho = synth.disk_density(J, K, L, 2, spiral=True, spectrum=True)
+    o.rho[...] = rho
+    dth = 2.0 * 3.1415926535897932 / L
+    for jmin in (1, 2, 7):
+        _, (ix, iy) = o.external_pot(mass_star=2.0, rpstar=0.01, phi_star=0.3, indirect=True, jmin=jmin)
+        psi = (np.arange(L) + 0.5) * dth
+        sub = rho[jmin - 1:J + 1, 1:K + 1, :]
+        r = np.asarray(o.rhf[jmin - 1:J + 1])[:, None, None]
+        m = sub * r * (1.0 / J) * (0.5 / K) * 2.0 * dth
+        sx = float(np.sum(m * np.cos(psi) * r))
+        sy = float(np.sum(m * np.sin(psi) * r))
+        assert ix == pytest.approx(-(0.01 * math.cos(0.3) + sx) / 2.0, rel=1e-13)
+        assert iy == pytest.approx(-(0.01 * math.sin(0.3) + sy) / 2.0, rel=1e-13)
+
+
+# ---------------------------------------------------------------------------
+# SOURCE's potential, pressure and rotation terms (radhydro/source.f:45-81)
+# ---------------------------------------------------------------------------
+def test_source_terms_match_numpy_and_conserve(ora):
+    """The oracle's S, T, A updates against a numpy statement of the same
+    differences (exact in this order of operations), and the A update's sum
+    over L of the pressure part vanishes (periodic differences)."""
+    J, K, L = 12, 6, 8
+    rng = np.random.default_rng(4)
+    hs = (J + 2, K + 2, L)
+    rho, phi, omega, p = (np.asfortranarray(rng.random(hs)) for _ in range(4))
+    s, t, a = (np.asfortranarray(rng.random(hs)) for _ in range(3))
+    s0, t0, a0 = s.copy(), t.copy(), a.copy()
+    r = (np.arange(1, J + 3) - 2) * 0.1
+    dr, dz, dth, delt = 0.1, 0.05, 2 * np.pi / L, 1e-3
+    ora.source(r, rho, phi, omega, p, s, t, a, delt, dr, dz, dth, jmin=2)
+    j = slice(2, J + 1)          # J = 3..JMAX1 (0-based 2..J)
+    jm = slice(1, J)
+    k = slice(1, K + 1)
+    rs = rho[j, k] + rho[jm, k]
+    om = omega[j, k] + omega[jm, k]
+    want_s = s0[j, k] + delt * (r[j, None, None] * rs * (om * om) * 0.25 * 0.5 -
+                                rs * (phi[j, k] - phi[jm, k]) / (2 * dr) - (p[j, k] - p[jm, k]) / dr)
+    assert np.array_equal(s[j, k], want_s)
+    jj = slice(1, J + 1)
+    km = slice(0, K)
+    want_t = t0[jj, k] - delt * (0.5 * (rho[jj, k] + rho[jj, km]) * (phi[jj, k] - phi[jj, km]) / dz +
+                                 (p[jj, k] - p[jj, km]) / dz)
+    assert np.array_equal(t[jj, k], want_t)
+    lp, lm = np.roll(np.arange(L), -1), np.roll(np.arange(L), 1)
+    want_a = a0[jj, k] - delt * (rho[jj, k] * (phi[jj, k][:, :, lp] - phi[jj, k][:, :, lm]) +
+                                 p[jj, k][:, :, lp] - p[jj, k][:, :, lm]) / (2 * dth)
+    assert np.array_equal(a[jj, k], want_a)
+    # untouched: J = 1 and 2 of S, K = 1 and KMAX+2 everywhere
+    assert np.array_equal(s[:2], s0[:2]) and np.array_equal(t[:, 0], t0[:, 0])
+    assert np.array_equal(a[:, K + 1], a0[:, K + 1])
