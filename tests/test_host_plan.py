@@ -126,3 +126,18 @@ def test_status_strings_and_argument_checks(chylib):
     assert L.chy_plan_create(C.byref(g), 7, 1, C.byref(p)) == 10
     assert L.chy_plan_create(C.byref(g), 0, 0, C.byref(p)) == 10
     assert L.chy_solve(None, None, None, None, 0, None) == 10
+
+
+def test_external_and_source_argument_checks(chylib):
+    """The star-potential and SOURCE entry points reject null plans and
+    arguments before touching the device."""
+    L = chylib.lib()
+    e = chylib.ChyExternal(1.0, 0.0, 0.0, 0.0, 0, 2)
+    assert L.chy_plan_set_external(None, C.byref(e)) == 10
+    assert L.chy_plan_set_external(None, None) == 10
+    assert L.chy_plan_star_potential(None, None, 0, None) == 10
+    a = chylib.ChySourceArgs()
+    assert L.chy_source(None, C.byref(a), None) == 10
+    assert L.chy_source(None, None, None) == 10
+    assert C.sizeof(chylib.ChyDiag) == 8 + 8 + 4 + 4 + 64 + 16
+    assert C.sizeof(chylib.ChyExternal) == 4 * 8 + 2 * 4
