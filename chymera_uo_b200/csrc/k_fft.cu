@@ -457,6 +457,37 @@ __global__ void k_coef(DevTables t, Work w)
 // ghosts (pot/pot3.f:289-292) and the ZAXPHI row PHI(JMAX+2, K, :)
 // (pot/pot3.f:350-387); CTAs at K = 2 write the midplane ghosts
 // (pot/pot3.f:293-296).
+// ZAXPHI's Neville extrapolation to r = 0 (pot/pot3.f:354-378) for azimuth
+// l from NP samples PHI(2.., K, L) and PHI(2.., K, L+N) at the abscissae ZX,
+// every operation as the reference orders it.  The table P2 is held as its
+// live tail Q(S) = P2(II+S), which shifts down one place per step II, so
+// that every index is static and the table stays in registers.
+template <int NP, class F>
+__device__ __forceinline__ double neville_axis(const double (&zx)[11], F sample, int l, int lm)
+{
+    constexpr int ichk = NP % 2, num = (NP - ichk) / 2, jsp = num + 1;
+    double q[NP];   // q[i] = P2(i + 1) before the first step
+#pragma unroll
+    for (int jj = 2; jj <= jsp; ++jj) {
+        q[num + (jj - 1) - 1] = sample(l, jj - 2);
+        q[num - (jj - 2) - 1] = sample(l + lm, jj - 2);
+    }
+    if constexpr (ichk == 1) q[num + num] = sample(l, num);
+    const double xpoint = 0.0;
+#pragma unroll 1
+    for (int ii = 1; ii <= NP - 1; ++ii) {
+        const double p1 = q[0], xinv = 1.0 / zx[ii], xr = xpoint * xinv;
+#pragma unroll
+        for (int s = 0; s < NP - 1; ++s) {
+            if (s < NP - ii) {   // JJ = II + 1 + S
+                const double xratio = zx[ii + 1 + s] * xinv, pp = q[s + 1];
+                q[s] = (p1 * (xratio - xr) + pp * (xr - 1.0)) / (xratio - 1.0);
+            }
+        }
+    }
+    return q[0];
+}
+
 // STARPHI of the cell (j, k, l) of PHI(J+2, K+2, L), 0-based, with the star at
 // (ix, iy): the reference's expression in its order of operations, every
 // product and sum rounded on its own (pot/ExternalPot.f:44-49).  COS/SIN of
@@ -540,24 +571,20 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
             if (k == 0) phi[(size_t)J2 * ((size_t)K2 * l)] = out(0, 0, l, v);     // PHI(1,1,L)
         }
         // ZAXPHI: Neville extrapolation to r = 0 across +-RHF (pot/pot3.f:354-378)
-        const int lm = L / 2, np = t.npoint;
-        const int ichk = np % 2, num = (np - ichk) / 2, jsp = num + 1;
+        const int lm = L / 2;
         for (int l = threadIdx.x; l < lm; l += blockDim.x) {
-            double p2[11];
-            for (int jj = 2; jj <= jsp; ++jj) {
-                p2[num + (jj - 1)] = sample(l, jj - 2);
-                p2[num - (jj - 2)] = sample(l + lm, jj - 2);
+            double ph;
+            switch (t.npoint) {   // 2..10, checked at plan creation
+            case 2: ph = neville_axis<2>(t.zx, sample, l, lm); break;
+            case 3: ph = neville_axis<3>(t.zx, sample, l, lm); break;
+            case 4: ph = neville_axis<4>(t.zx, sample, l, lm); break;
+            case 5: ph = neville_axis<5>(t.zx, sample, l, lm); break;
+            case 6: ph = neville_axis<6>(t.zx, sample, l, lm); break;
+            case 7: ph = neville_axis<7>(t.zx, sample, l, lm); break;
+            case 8: ph = neville_axis<8>(t.zx, sample, l, lm); break;
+            case 9: ph = neville_axis<9>(t.zx, sample, l, lm); break;
+            default: ph = neville_axis<10>(t.zx, sample, l, lm); break;
             }
-            if (ichk == 1) p2[num + num + 1] = sample(l, num);
-            const double xpoint = 0.0;
-            for (int ii = 1; ii <= np - 1; ++ii) {
-                const double p1 = p2[ii], xinv = 1.0 / t.zx[ii], xr = xpoint * xinv;
-                for (int jj = ii + 1; jj <= np; ++jj) {
-                    const double xratio = t.zx[jj] * xinv, pp = p2[jj];
-                    p2[jj] = (p1 * (xratio - xr) + pp * (xr - 1.0)) / (xratio - 1.0);
-                }
-            }
-            const double ph = p2[np];
             red[l] = ph;
             phi[(size_t)(t.J + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] = out(t.J + 1, k + 1, l, ph);
             phi[(size_t)(t.J + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * (l + lm))] = out(t.J + 1, k + 1, l + lm, ph);
