@@ -19,15 +19,18 @@
 
 namespace chy {
 
-// Grid: (nsub, 1, ceil(batch / kSubBatch)), 256 threads.  The ring-table
-// slice of a sub-chunk is loaded once and serves up to kSubBatch solves.
+// Grid: (nsub, 1, ceil(batch / kSubBatch)).  The ring-table slice of a
+// sub-chunk is loaded once and serves up to kSubBatch solves; when the 2*ncol
+// column sums of one solve fill at most half the block, two solves are summed
+// side by side.  Every column sum keeps its order, whatever the pairing.
 constexpr int kSubBatch = 8;
-__global__ void __launch_bounds__(256) k_bdy_sub(DevTables t, Work w, int nb)
+constexpr int kSubThreads = 512;
+__global__ void __launch_bounds__(kSubThreads) k_bdy_sub(DevTables t, Work w, int nb, int spp)
 {
     extern __shared__ double smem[];
-    const int RL = t.srow, NT_ = t.ntrm;
+    const int RL = t.srow, NT_ = t.ntrm, per = 2 * t.ncol;
     double *s_row = smem;                                      // [ns][RL]: TERM, r^-(2l+1), DV
-    double (*s_mom)[21] = reinterpret_cast<double (*)[21]>(smem + kSubChunk * RL);
+    double *s_mom = smem + kSubChunk * RL;                     // [spp][ns][21]
     const int sc = blockIdx.x;
     const int s0 = t.sub_start[sc], s1 = t.sub_start[sc + 1], ns = s1 - s0;
 
@@ -35,28 +38,31 @@ __global__ void __launch_bounds__(256) k_bdy_sub(DevTables t, Work w, int nb)
     // r^-(2l+1) of :587, DV of :516)
     for (int i = threadIdx.x; i < ns * RL; i += blockDim.x) s_row[i] = t.sterm[(size_t)s0 * RL + i];
     const int b0 = blockIdx.z * kSubBatch, b1 = min(nb, b0 + kSubBatch);
-    for (int b = b0; b < b1; ++b) {
-        __syncthreads();   // s_row loaded / s_mom of the previous solve consumed
-        // DV * moments of this solve
-        const double *mom = w.mom + (size_t)b * w.smom;
-        for (int it = threadIdx.x; it < ns * 21; it += blockDim.x) {
-            const int r = it / 21, q = it % 21;
-            s_mom[r][q] = s_row[r * RL + NT_ + 11] * mom[(size_t)q * t.nring + t.ring_sorted[s0 + r]];
+    for (int b = b0; b < b1; b += spp) {
+        const int nsl = min(spp, b1 - b);
+        __syncthreads();   // s_row loaded / s_mom of the previous solves consumed
+        // DV * moments of these solves
+        for (int it = threadIdx.x; it < nsl * ns * 21; it += blockDim.x) {
+            const int sl = it / (ns * 21), rq = it % (ns * 21), r = rq / 21, q = rq % 21;
+            const double *mom = w.mom + (size_t)(b + sl) * w.smom;
+            s_mom[((size_t)sl * kSubChunk + r) * 21 + q] =
+                s_row[r * RL + NT_ + 11] * mom[(size_t)q * t.nring + t.ring_sorted[s0 + r]];
         }
         __syncthreads();
-        double *sub = w.sub + (size_t)b * w.ssub + (size_t)sc * 2 * t.ncol;
-        for (int cc = threadIdx.x; cc < 2 * t.ncol; cc += blockDim.x) {
+        for (int task = threadIdx.x; task < nsl * per; task += blockDim.x) {
+            const int sl = task / per, cc = task % per;
             const int col = cc % t.ncol, out = cc / t.ncol;
             const int term = t.col_term[col], m = t.col_m[col], l = t.col_l[col];
             const int mq = t.col_part[col] == 0 ? m : 10 + m;
+            const double *sm = s_mom + (size_t)sl * kSubChunk * 21;
             double acc = 0.0;
             if (!out) {
-                for (int r = 0; r < ns; ++r) acc = acc + s_row[r * RL + term] * s_mom[r][mq];
+                for (int r = 0; r < ns; ++r) acc = acc + s_row[r * RL + term] * sm[r * 21 + mq];
             } else {
                 for (int r = 0; r < ns; ++r)
-                    acc = acc + (s_row[r * RL + term] * s_mom[r][mq]) * s_row[r * RL + NT_ + l];
+                    acc = acc + (s_row[r * RL + term] * sm[r * 21 + mq]) * s_row[r * RL + NT_ + l];
             }
-            sub[(size_t)out * t.ncol + col] = acc;
+            w.sub[(size_t)(b + sl) * w.ssub + (size_t)sc * 2 * t.ncol + (size_t)out * t.ncol + col] = acc;
         }
     }
 }
@@ -113,10 +119,14 @@ __global__ void __launch_bounds__(256) k_bdy_scan(DevTables t, Work w)
 
 cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStream_t s)
 {
-    const size_t sm = (size_t)kSubChunk * (t.srow + 21) * sizeof(double);
+    // two solves per pass when there are two and a solve's column sums fill
+    // at most half the block
+    const int per = 2 * t.ncol, spp = (nb >= 2 && 2 * per <= kSubThreads) ? 2 : 1;
+    const int threads = spp == 2 ? ((2 * per + 31) / 32) * 32 : 256;
+    const size_t sm = (size_t)kSubChunk * (t.srow + 21 * spp) * sizeof(double);
     cudaError_t e = ensure_smem((const void *)k_bdy_sub, sm);
     if (e != cudaSuccess) return e;
-    k_bdy_sub<<<dim3(t.nsub, 1, (nb + kSubBatch - 1) / kSubBatch), 256, sm, s>>>(t, w, nb);
+    k_bdy_sub<<<dim3(t.nsub, 1, (nb + kSubBatch - 1) / kSubBatch), threads, sm, s>>>(t, w, nb, spp);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_bdy_scan<<<dim3(2 * t.ncol, 1, nb), 256, 0, s>>>(t, w);
