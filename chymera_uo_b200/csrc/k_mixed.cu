@@ -20,6 +20,8 @@
 // No TMA multicast is used anywhere.  Every wait is bounded: on a timeout the
 // kernel records an error word, stops issuing work, releases its tensor
 // memory and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -47,6 +49,9 @@ constexpr int kResY = 128 * kResYS, kResBuf = kResY + 130 * kResXS;
 constexpr int kEpiD = 128 * 33;
 // resident-iterate residual: three-deep ring of 32-column chunks, row stride 34
 constexpr int kRingC = 32, kRingS = 34, kRingBuf = 128 * kRingS;
+// tensor-map ring: a slot is two 16-column halves of 128 rows x 128 bytes
+constexpr int kRingHalf = 128 * 128, kRingSlot = 2 * kRingHalf;
+static_assert(3 * kRingSlot <= 3 * kRingBuf * 8, "ring fits the staging region");
 constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
 constexpr size_t kStageBytes =
     cmax(cmax((size_t)(kEpiD + 2 * 128 * 32) * 8, (size_t)2 * kResBuf * 8), (size_t)3 * kRingBuf * 8);
@@ -84,6 +89,8 @@ struct MixedState {
     double *h_corr = nullptr;       // pinned [max_batch][L][8][2]
     size_t xbuf_bytes = 0;          // FP64 iterate (two or more corrections)
     int *h_err = nullptr;           // pinned
+    CUtensorMap tm_x{};             // X as rows of JMAX doubles: 16 x KMAX tiles, 128-byte swizzle
+    bool tm_ok = false;
 };
 
 // ---------------------------------------------------------------------------
@@ -103,6 +110,11 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
 __device__ __forceinline__ void mbar_init(uint64_t *bar, int count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
@@ -134,6 +146,17 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+
+// One 2-D tile of the tensor map at (x, y) into shared memory, counted on bar.
+// No multicast.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
 }
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -374,7 +397,8 @@ struct MixedSmem {
 // FP64 iterate never goes through global memory.  Otherwise (more
 // corrections) the iterate is kept in FP64 in x.xbuf.
 template <bool kRes>
-__global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, MixedDev x, int nb)
+__global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, MixedDev x, int nb,
+                                                     const __grid_constant__ CUtensorMap tm_x)
 {
     extern __shared__ __align__(1024) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -392,7 +416,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     float *f_edge = f_xch + 512;                                               // [2][8][2][16]
     uint64_t *bar_mma = reinterpret_cast<uint64_t *>(f_edge + 512);
     uint64_t *bar_a = bar_mma + 1;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_a + 1);
+    uint64_t *bar_ring = bar_a + 1;   // [3] residual ring slots
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_ring + 3);
     int *s_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
     // ---- setup: tensor memory (all 512 columns), barriers, m-independent tables
@@ -403,6 +428,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     if (tid == 0) {
         mbar_init(bar_mma, 1);
         mbar_init(bar_a, 1);
+        for (int i = 0; i < 3; ++i) mbar_init(bar_ring + i, 1);
         *s_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -429,6 +455,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     const uint32_t idesc = (1u << 4) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
     const int nit = kRes ? min(x.nit, 2) : x.nit;
     uint32_t ph_mma = 0, ph_a = 0;
+    uint32_t ring_ph = 0, ring_pend = 0;   // residual ring slots: phase parity, copies in flight
     bool failed = false;
 
     const long long items = (long long)nb * t.L;
@@ -494,25 +521,61 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             float rmax = 0.0f;
             if constexpr (kRes) {
                 // Raw X rows k = 0..KMAX-1 (boundary row NZ and column M
-                // included) stream through a three-deep cp.async ring of
-                // 32-column chunks; x0 comes from tensor memory, its vertical
-                // neighbours by warp shuffles and, across warps, through
-                // shared memory.  Row stride 17 granules: the 16-byte reads of
-                // eight consecutive rows fall on distinct banks.
-                double *ring = reinterpret_cast<double *>(sBh);
+                // included) stream through a three-deep ring of 32-column
+                // chunks loaded by the tensor-memory-access engine: per chunk
+                // two 16-column x KMAX-row tiles of the tensor map over X, in
+                // the 128-byte swizzle (16-byte granule g of row k at
+                // g ^ (k % 8)), so the 16-byte reads of eight consecutive rows
+                // fall on distinct banks.  x0 comes from tensor memory, its
+                // vertical neighbours by warp shuffles and, across warps,
+                // through shared memory.
+                uint8_t *ring = sBh;                       // [3][2][128 rows][128 B]
                 const int nchr = NT / kRingC;
+                const int row0 = (b * t.L + l) * K;        // first tensor-map row of this item
+                // thread 0 issues chunk c into slot c % 3 (after the barrier
+                // that retired the slot's previous chunk); halves past JMAX
+                // are zero-filled instead
                 auto issue = [&](int c) {
-                    if (c < nchr) {
-                        double *sy = ring + (c % 3) * kRingBuf;
-                        const int c0 = c * kRingC;
-                        for (int g = tid; g < K * (kRingC / 2); g += 256) {
-                            const int k = g >> 4, q = g & 15, j = c0 + 2 * q;
-                            const bool ok = j < J;
-                            cp_async16(sy + k * kRingS + 2 * q, ok ? Xl + (size_t)k * J + j : Xl, ok ? 16 : 0);
+                    if (c >= nchr) return;
+                    ring_pend |= 1u << (c % 3);
+                    if (warp != 0) return;
+                    const int sl = c % 3, c0 = c * kRingC;
+                    uint8_t *slot = ring + sl * kRingSlot;
+                    const int halves = c0 >= J ? 0 : (c0 + 16 >= J ? 1 : 2);
+                    if (lane == 0) {
+                        if (halves > 0) {
+                            mbar_expect_tx(bar_ring + sl, (uint32_t)(halves * K * 128));
+                            for (int h = 0; h < halves; ++h)
+                                tma_load_2d(slot + h * kRingHalf, &tm_x, c0 + 16 * h, row0, bar_ring + sl);
+                        } else {
+                            mbar_arrive(bar_ring + sl);
                         }
                     }
-                    cp_async_commit();
+                    for (int h = halves; h < 2; ++h)
+                        for (int i = lane; i < K * 16; i += 32)
+                            reinterpret_cast<double *>(slot + h * kRingHalf)[i] = 0.0;
                 };
+                // all threads: chunk c has landed (bounded wait; on a timeout
+                // the slot stays pending for the drain at the end)
+                auto landed = [&](int c) {
+                    const int sl = c % 3;
+                    if (mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u)) {
+                        ring_ph ^= 1u << sl;
+                        ring_pend &= ~(1u << sl);
+                    } else {
+                        *s_flag = 1;
+                    }
+                };
+                // element (row k, column cc < 32) of a slot
+                auto at = [&](const uint8_t *slot, int k, int cc) -> const double * {
+                    const int h = cc >> 4, q = cc & 15;
+                    return reinterpret_cast<const double *>(slot + h * kRingHalf + k * 128 +
+                                                            ((((q >> 1) ^ (k & 7))) << 4) + ((q & 1) << 3));
+                };
+                // generic writes to this region (splits, epilogue staging)
+                // are ordered before the copy engine's writes
+                fence_proxy_async();
+                __syncthreads();
                 issue(0);
                 issue(1);
                 const int k = kq, jb = jh * 16, quad = warp & 3;
@@ -527,7 +590,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                         tm_ld16_nw(tmem + lane_base + c0 + jb, xc);
                         tm_ld1_nw(tmem + lane_base + (uint32_t)(jl < 0 ? 0 : jl), xlf);
                         tm_ld1_nw(tmem + lane_base + (uint32_t)(jr < NT ? jr : NT - 1), xrt);
-                        cp_async_wait<1>();
+                        landed(c);
                         tm_wait_ld18(xc, xlf, xrt);
                         if (jl < 0) xlf = 0.f;
                         if (jr >= NT) xrt = 0.f;
@@ -541,33 +604,33 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                             for (int u = 0; u < 16; ++u) ed[16 + u] = xc[u];
                         }
                     } else {
-                        cp_async_wait<1>();
+                        landed(c);
                     }
                     __syncthreads();
+                    if (*s_flag) break;   // a tile did not land: stop (uniform)
                     issue(c + 2);
                     // right-hand side 4 pi G rho with the boundary folds
                     // (pot/pot3.f:219-224): the row below the top boundary folds
                     // row NZ (one thread), the column M fold lies in one chunk
-                    const double *buf = ring + (c % 3) * kRingBuf;
-                    const double *sy = buf + k * kRingS;
+                    const uint8_t *slot = ring + (c % 3) * kRingSlot;
                     double yv[16];
 #pragma unroll
                     for (int u = 0; u < 16; u += 2) {
-                        const double2 t2 = *reinterpret_cast<const double2 *>(sy + jb + u);
+                        const double2 t2 = *reinterpret_cast<const double2 *>(at(slot, k, jb + u));
                         yv[u] = t.pig4 * t2.x;
                         yv[u + 1] = t.pig4 * t2.y;
                     }
                     if (k == NZ - 1) {
 #pragma unroll
                         for (int u = 0; u < 16; u += 2) {
-                            const double2 t3 = *reinterpret_cast<const double2 *>(buf + NZ * kRingS + jb + u);
+                            const double2 t3 = *reinterpret_cast<const double2 *>(at(slot, NZ, jb + u));
                             yv[u] = fma(-t.cnmax, t3.x, yv[u]);
                             yv[u + 1] = fma(-t.cnmax, t3.y, yv[u + 1]);
                         }
                     }
                     const int uM = M - 1 - (c0 + jb);   // uniform in the warp
                     if (uM >= 0 && uM < 16) {
-                        const double yM = sy[M - c0];
+                        const double yM = *at(slot, k, M - c0);
 #pragma unroll
                         for (int u = 0; u < 16; ++u)
                             if (u == uM) yv[u] = fma(-t.cmmax, yM, yv[u]);
@@ -615,8 +678,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     }
                     tm_st16_nw(tmem + lane_base + 256 + c0 + jb, v);
                 }
-                cp_async_wait<0>();
                 tm_wait_st();
+                if (*s_flag) { failed = true; break; }
             } else {
                 // Chunks of kRC columns, double-buffered with cp.async: raw X
                 // rows k = 0..KMAX-1 and the iterate rows k = -1..NZ with
@@ -976,8 +1039,10 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             }
         }
     }
-    // drain a transfer still in flight, then release tensor memory
+    // drain transfers still in flight (bounded), then release tensor memory
     if (a_inflight && !failed) mbar_wait(bar_a, ph_a);
+    for (int sl = 0; sl < 3; ++sl)
+        if (ring_pend & (1u << sl)) mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u);
     if (failed && tid == 0) atomicExch(x.err, 1);
     tc_fence_before();
     __syncthreads();
@@ -1096,6 +1161,24 @@ size_t chy_mixed_work_doubles(const chy_plan *p)
     return (size_t)hp.L * 16 * p->max_batch + 8;
 }
 
+// cuTensorMapEncodeTiled from the driver, through the runtime (no link-time
+// dependency on the driver library).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
 void chy_mixed_bind_work(chy_plan *p, double *base)
 {
     if (!p->mx) p->mx = new MixedState();
@@ -1110,6 +1193,18 @@ void chy_mixed_bind_work(chy_plan *p, double *base)
     if (p->precision == CHY_PREC_MIXED) {
         cudaMallocHost(&p->mx->h_corr, sizeof(double) * d.scorr * p->max_batch);
         cudaMallocHost(&p->mx->h_err, sizeof(int));
+        // the residual's right-hand-side tiles: X viewed as max_batch*L*K rows
+        // of J doubles; one item is K consecutive rows
+        PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+        if (enc && hp.K <= 256 && hp.J % 16 == 0) {
+            const cuuint64_t dims[2] = {(cuuint64_t)hp.J, (cuuint64_t)p->max_batch * hp.L * hp.K};
+            const cuuint64_t strides[1] = {(cuuint64_t)hp.J * sizeof(double)};
+            const cuuint32_t box[2] = {16, (cuuint32_t)hp.K};
+            const cuuint32_t es[2] = {1, 1};
+            p->mx->tm_ok = enc(&p->mx->tm_x, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p->w.X, dims, strides, box, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        }
     }
 }
 
@@ -1125,13 +1220,14 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
         return CHY_ERR_ARG;
     const size_t sm = MixedSmem::bytes(d.ntile);
     // two approximate solves (one correction) keep the iterate in tensor memory
+    if (d.nit <= 2 && !p->mx->tm_ok) return CHY_ERR_CUDA;   // tensor map over X not encoded
     const void *kern = d.nit <= 2 ? (const void *)k_mode_mixed<true> : (const void *)k_mode_mixed<false>;
     cudaError_t e = ensure_smem(kern, sm);
     if (e != cudaSuccess) return CHY_ERR_CUDA;
     const long long items = (long long)nb * p->hp.L;
     const int grid = (int)(items < p->num_sms ? items : p->num_sms);
-    if (d.nit <= 2) k_mode_mixed<true><<<grid, 256, sm, s>>>(p->t, p->w, d, nb);
-    else k_mode_mixed<false><<<grid, 256, sm, s>>>(p->t, p->w, d, nb);
+    if (d.nit <= 2) k_mode_mixed<true><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x);
+    else k_mode_mixed<false><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x);
     if (cudaGetLastError() != cudaSuccess) return CHY_ERR_CUDA;
     *launches = 1;
     return CHY_OK;
