@@ -488,7 +488,11 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     };
 
     for (long long item = blockIdx.x; item < items && !failed; item += gridDim.x) {
-        const int b = (int)(item / t.L), l = (int)(item % t.L);
+        // mode-major order, modes l and l + N (same m) side by side and the
+        // batch's solves innermost: the items in flight at once share a few
+        // sweep-table slices, which then stay in L2
+        const int o = (int)(item / nb), b = (int)(item % nb);
+        const int l = (o & 1) ? (o >> 1) + t.N : (o >> 1);
         const int m = l <= t.N ? l : l - t.N;
         const double xl2 = 2.0 * (t.xlamm[m] - 1.0);
         // BM_m (pot/pot3.f:226-230) for the FP64 residual (the sweeps use the
