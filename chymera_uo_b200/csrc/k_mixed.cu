@@ -90,6 +90,7 @@ struct MixedState {
     size_t xbuf_bytes = 0;          // FP64 iterate (two or more corrections)
     int *h_err = nullptr;           // pinned
     CUtensorMap tm_x{};             // X as rows of JMAX doubles: 16 x KMAX tiles, 128-byte swizzle
+    CUtensorMap tm_xs{};            // the same with 16 x (KMAX-1) tiles: stores skip the boundary row
     bool tm_ok = false;
 };
 
@@ -158,6 +159,22 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
+
+// One 2-D tile from shared memory to the tensor map at (x, y), in the
+// thread's bulk async-group.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, int x, int y, const void *src)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// at most N of this thread's bulk groups still reading shared memory
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory"); }
+// all of this thread's bulk groups complete (writes performed)
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -398,7 +415,8 @@ struct MixedSmem {
 // corrections) the iterate is kept in FP64 in x.xbuf.
 template <bool kRes>
 __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, MixedDev x, int nb,
-                                                     const __grid_constant__ CUtensorMap tm_x)
+                                                     const __grid_constant__ CUtensorMap tm_x,
+                                                     const __grid_constant__ CUtensorMap tm_xs)
 {
     extern __shared__ __align__(1024) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -510,6 +528,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
         double *xl = kRes ? nullptr : x.xbuf + (size_t)b * x.sxb + (size_t)l * K * J;
         double *cr = x.corr + (size_t)b * x.scorr + (size_t)l * 16;
         double u0 = 0.0;   // kRes: scale of x0 held in tensor memory
+        double ym_keep = 0.0;   // kRes: X(k, M) of this thread's row, for the write-back tiles
         __syncthreads();
 
         for (int it = 0; it < nit && !failed; ++it) {
@@ -635,6 +654,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     const int uM = M - 1 - (c0 + jb);   // uniform in the warp
                     if (uM >= 0 && uM < 16) {
                         const double yM = *at(slot, k, M - c0);
+                        ym_keep = yM;
 #pragma unroll
                         for (int u = 0; u < 16; ++u)
                             if (u == uM) yv[u] = fma(-t.cmmax, yM, yv[u]);
@@ -936,44 +956,52 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     u0 = unscale;   // x0 stays in tensor memory columns [0, NT)
                     continue;
                 }
-                // X = x0 + delta (FP64), staged through sD[buf][k][jj] to write
-                // rows; the next chunk's tensor-memory rows load while this
-                // chunk's rows are stored
+                // X = x0 + delta (FP64).  Each 32-column chunk is staged in
+                // one of three slots (two 16-column halves, 128-byte swizzle)
+                // and written by the copy engine as tiles of rows 0..KMAX-2
+                // (the boundary row is not written); column M, which shares
+                // the last tile, carries X's own value back.  The next chunk's
+                // tensor-memory rows load while this chunk's tiles are stored.
                 double sd = 0.0, sx = 0.0;
-                const int jb = jh * 16;
+                const int jb = jh * 16, row0 = (b * t.L + l) * K;
                 float dv[16], xv[16];
                 tm_ld16_nw(tmem + lane_base + acc + jb, dv);
                 if (res_x) tm_ld16_nw(tmem + lane_base + jb, xv);
-                for (int c0 = 0; c0 < NT; c0 += 32) {
-                    double *sD = reinterpret_cast<double *>(sBh) + ((c0 >> 5) & 1) * (128 * 34);
+                for (int c0 = 0, c = 0; c0 < NT; c0 += 32, ++c) {
+                    uint8_t *slot = sBh + (c % 3) * kRingSlot;
                     tm_wait_ld32(dv, xv);
+                    double xn[16];
 #pragma unroll
                     for (int u = 0; u < 16; ++u) {
                         const int j = c0 + jb + u;
                         const double dl = (double)dv[u] * unscale;
-                        const double xn = (res_x ? (double)xv[u] * u0 : 0.0) + dl;
-                        sD[kq * 34 + jb + u] = xn;
+                        xn[u] = (res_x ? (double)xv[u] * u0 : 0.0) + dl;
                         if (kq < NZ && j < M) {
                             sd += dl * dl;
-                            sx += xn * xn;
+                            sx += xn[u] * xn[u];
                         }
+                        if (j == M) xn[u] = ym_keep;   // column M (uniform in the warp)
                     }
+#pragma unroll
+                    for (int u = 0; u < 16; u += 2) {
+                        const int q = jb + u, h = q >> 4, g = (q & 15) >> 1;
+                        *reinterpret_cast<double2 *>(slot + h * kRingHalf + kq * 128 + ((g ^ (kq & 7)) << 4)) =
+                            make_double2(xn[u], xn[u + 1]);
+                    }
+                    fence_proxy_async();
+                    if (tid == 0) bulk_wait_read<1>();   // the store from this slot's last chunk has read it
                     __syncthreads();
                     if (c0 + 32 < NT) {
                         tm_ld16_nw(tmem + lane_base + acc + c0 + 32 + jb, dv);
                         if (res_x) tm_ld16_nw(tmem + lane_base + c0 + 32 + jb, xv);
                     }
-                    // rows of X in 16-byte pieces (J even: pieces never straddle
-                    // column M, which only the last piece of a row touches)
-                    for (int i = tid; i < 128 * 16; i += 256) {
-                        const int k = i >> 4, jj = 2 * (i & 15), j = c0 + jj;
-                        if (k >= NZ || j >= M) continue;
-                        const double2 val = *reinterpret_cast<const double2 *>(sD + k * 34 + jj);
-                        double *dst = Xl + (size_t)k * J + j;
-                        if (j + 1 < M) *reinterpret_cast<double2 *>(dst) = val;
-                        else *dst = val.x;
+                    if (tid == 0) {
+                        for (int h = 0; h < 2 && c0 + 16 * h < J; ++h)
+                            tma_store_2d(&tm_xs, c0 + 16 * h, row0, slot + h * kRingHalf);
+                        bulk_commit();
                     }
                 }
+                if (tid == 0) bulk_wait_all();   // tiles written, staging free for the next item
                 __syncthreads();
                 block_sum3(sd, sx, (double)sxf);
                 if (tid == 0) {
@@ -1203,9 +1231,12 @@ void chy_mixed_bind_work(chy_plan *p, double *base)
         if (enc && hp.K <= 256 && hp.J % 16 == 0) {
             const cuuint64_t dims[2] = {(cuuint64_t)hp.J, (cuuint64_t)p->max_batch * hp.L * hp.K};
             const cuuint64_t strides[1] = {(cuuint64_t)hp.J * sizeof(double)};
-            const cuuint32_t box[2] = {16, (cuuint32_t)hp.K};
+            const cuuint32_t box[2] = {16, (cuuint32_t)hp.K}, box_s[2] = {16, (cuuint32_t)(hp.K - 1)};
             const cuuint32_t es[2] = {1, 1};
             p->mx->tm_ok = enc(&p->mx->tm_x, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p->w.X, dims, strides, box, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+                           enc(&p->mx->tm_xs, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p->w.X, dims, strides, box_s, es,
                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         }
@@ -1230,8 +1261,8 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
     if (e != cudaSuccess) return CHY_ERR_CUDA;
     const long long items = (long long)nb * p->hp.L;
     const int grid = (int)(items < p->num_sms ? items : p->num_sms);
-    if (d.nit <= 2) k_mode_mixed<true><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x);
-    else k_mode_mixed<false><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x);
+    if (d.nit <= 2) k_mode_mixed<true><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x, p->mx->tm_xs);
+    else k_mode_mixed<false><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x, p->mx->tm_xs);
     if (cudaGetLastError() != cudaSuccess) return CHY_ERR_CUDA;
     *launches = 1;
     return CHY_OK;
