@@ -49,12 +49,13 @@ constexpr int kResY = 128 * kResYS, kResBuf = kResY + 130 * kResXS;
 constexpr int kEpiD = 128 * 33;
 // resident-iterate residual: three-deep ring of 32-column chunks, row stride 34
 constexpr int kRingC = 32, kRingS = 34, kRingBuf = 128 * kRingS;
-// tensor-map ring: a slot is two 16-column halves of 128 rows x 128 bytes
-constexpr int kRingHalf = 128 * 128, kRingSlot = 2 * kRingHalf;
-static_assert(3 * kRingSlot <= 3 * kRingBuf * 8, "ring fits the staging region");
+// tensor-map ring: kRingSlots slots, each two 16-column halves of 128 rows x
+// 128 bytes
+constexpr int kRingHalf = 128 * 128, kRingSlot = 2 * kRingHalf, kRingSlots = 4;
 constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
-constexpr size_t kStageBytes =
-    cmax(cmax((size_t)(kEpiD + 2 * 128 * 32) * 8, (size_t)2 * kResBuf * 8), (size_t)3 * kRingBuf * 8);
+constexpr size_t kStageBytes = cmax(cmax(cmax((size_t)(kEpiD + 2 * 128 * 32) * 8, (size_t)2 * kResBuf * 8),
+                                         (size_t)3 * kRingBuf * 8),
+                                    (size_t)kRingSlots * kRingSlot);   // tensor-map ring
 static_assert((kRingBuf * 8) % 16 == 0, "16-byte staging");
 static_assert((kEpiD * 8) % 16 == 0 && (kResY * 8) % 16 == 0 && (kResBuf * 8) % 16 == 0, "16-byte staging");
 
@@ -434,8 +435,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     float *f_edge = f_xch + 512;                                               // [2][8][2][16]
     uint64_t *bar_mma = reinterpret_cast<uint64_t *>(f_edge + 512);
     uint64_t *bar_a = bar_mma + 1;
-    uint64_t *bar_ring = bar_a + 1;   // [3] residual ring slots
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_ring + 3);
+    uint64_t *bar_ring = bar_a + 1;   // [kRingSlots] residual ring slots
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_ring + kRingSlots);
     int *s_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
     // ---- setup: tensor memory (all 512 columns), barriers, m-independent tables
@@ -446,7 +447,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     if (tid == 0) {
         mbar_init(bar_mma, 1);
         mbar_init(bar_a, 1);
-        for (int i = 0; i < 3; ++i) mbar_init(bar_ring + i, 1);
+        for (int i = 0; i < kRingSlots; ++i) mbar_init(bar_ring + i, 1);
         *s_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -544,7 +545,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             float rmax = 0.0f;
             if constexpr (kRes) {
                 // Raw X rows k = 0..KMAX-1 (boundary row NZ and column M
-                // included) stream through a three-deep ring of 32-column
+                // included) stream through a four-deep ring of 32-column
                 // chunks loaded by the tensor-memory-access engine: per chunk
                 // two 16-column x KMAX-row tiles of the tensor map over X, in
                 // the 128-byte swizzle (16-byte granule g of row k at
@@ -552,17 +553,17 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 // fall on distinct banks.  x0 comes from tensor memory, its
                 // vertical neighbours by warp shuffles and, across warps,
                 // through shared memory.
-                uint8_t *ring = sBh;                       // [3][2][128 rows][128 B]
+                uint8_t *ring = sBh;                       // [kRingSlots][2][128 rows][128 B]
                 const int nchr = NT / kRingC;
                 const int row0 = (b * t.L + l) * K;        // first tensor-map row of this item
-                // thread 0 issues chunk c into slot c % 3 (after the barrier
-                // that retired the slot's previous chunk); halves past JMAX
-                // are zero-filled instead
+                // thread 0 issues chunk c into slot c % kRingSlots (after the
+                // barrier that retired the slot's previous chunk); halves past
+                // JMAX are zero-filled instead
                 auto issue = [&](int c) {
                     if (c >= nchr) return;
-                    ring_pend |= 1u << (c % 3);
+                    ring_pend |= 1u << (c % kRingSlots);
                     if (warp != 0) return;
-                    const int sl = c % 3, c0 = c * kRingC;
+                    const int sl = c % kRingSlots, c0 = c * kRingC;
                     uint8_t *slot = ring + sl * kRingSlot;
                     const int halves = c0 >= J ? 0 : (c0 + 16 >= J ? 1 : 2);
                     if (lane == 0) {
@@ -581,7 +582,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 // all threads: chunk c has landed (bounded wait; on a timeout
                 // the slot stays pending for the drain at the end)
                 auto landed = [&](int c) {
-                    const int sl = c % 3;
+                    const int sl = c % kRingSlots;
                     if (mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u)) {
                         ring_ph ^= 1u << sl;
                         ring_pend &= ~(1u << sl);
@@ -599,8 +600,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 // are ordered before the copy engine's writes
                 fence_proxy_async();
                 __syncthreads();
-                issue(0);
-                issue(1);
+                for (int c = 0; c < kRingSlots - 1; ++c) issue(c);
                 const int k = kq, jb = jh * 16, quad = warp & 3;
                 const bool krow = k < NZ;
                 const double an = d_an[k], cn = d_cn[k], bnk = d_bn[k];
@@ -631,11 +631,11 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     }
                     __syncthreads();
                     if (*s_flag) break;   // a tile did not land: stop (uniform)
-                    issue(c + 2);
+                    issue(c + kRingSlots - 1);
                     // right-hand side 4 pi G rho with the boundary folds
                     // (pot/pot3.f:219-224): the row below the top boundary folds
                     // row NZ (one thread), the column M fold lies in one chunk
-                    const uint8_t *slot = ring + (c % 3) * kRingSlot;
+                    const uint8_t *slot = ring + (c % kRingSlots) * kRingSlot;
                     double yv[16];
 #pragma unroll
                     for (int u = 0; u < 16; u += 2) {
@@ -1073,7 +1073,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     }
     // drain transfers still in flight (bounded), then release tensor memory
     if (a_inflight && !failed) mbar_wait(bar_a, ph_a);
-    for (int sl = 0; sl < 3; ++sl)
+    for (int sl = 0; sl < kRingSlots; ++sl)
         if (ring_pend & (1u << sl)) mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u);
     if (failed && tid == 0) atomicExch(x.err, 1);
     tc_fence_before();
