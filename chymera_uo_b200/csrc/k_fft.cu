@@ -8,7 +8,7 @@
 // moments, boundary synthesis).
 //
 // One CTA owns TC adjacent (J,K) columns and holds their LMAX samples in
-// shared memory as rows of stride RS = TC+1 doubles: row 2q is Re(z_q) and
+// shared memory as rows of stride RS = TC+2 doubles: row 2q is Re(z_q) and
 // row 2q+1 is Im(z_q) of the LMAX/2-point complex sequence
 // z_q = rho(2q) + i rho(2q+1) that POT3 builds (pot/pot3.f:95-98).  Global
 // loads and stores run along J, the fastest dimension of the reference's
@@ -55,7 +55,7 @@ template <int L>
 struct Tile {
     static constexpr int N = L / 2;
     static constexpr int TC = L <= 128 ? 32 : (L <= 256 ? 16 : 8);  // columns per CTA
-    static constexpr int RS = TC + 1;                               // row stride (doubles)
+    static constexpr int RS = TC + 2;                               // row stride (doubles, even)
     static constexpr int ROWS = L + 2;
     static constexpr int TPC = 256 / TC;                            // threads per column
 };
@@ -74,6 +74,12 @@ struct FftSmem {
 __device__ __forceinline__ void cp_async8(void *dst, const void *src, int bytes)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
                  "l"(src), "r"(bytes)
                  : "memory");
 }
@@ -257,12 +263,17 @@ __device__ __forceinline__ void realtr_pairs(double *A, const FftSmem &s)
 // POT3 copies into PHI (pot/pot3.f:70-82) and BDYGEN integrates
 // (pot/boundary.f:366-370) -- and writes X interior plus MOM.
 template <int L>
-__global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work w)
+__global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work w, int vec16)
 {
     using T = Tile<L>;
     extern __shared__ __align__(16) char smem_raw[];
-    double *A = (double *)smem_raw;
-    double *mtab = A + (size_t)T::ROWS * T::RS;            // [20][L/4] cos, sin of m psi
+    // Row l of the tile holds RHO(J0+1 .. J0+TC+2, K, L) at columns -1 .. TC:
+    // the view A is shifted by one element, so A[l*RS + c] is column
+    // j = j0 + c (RHO(j + 2, ...)), and the 16-byte granules of a row start
+    // on 16-byte boundaries (RS even).
+    double *A0 = (double *)smem_raw;
+    double *A = A0 + 1;
+    double *mtab = A0 + (size_t)T::ROWS * T::RS;           // [20][L/4] cos, sin of m psi
     FftSmem fs = carve_fft<L>((char *)(mtab + 20 * (L / 4)));
     const int J2 = t.J + 2, K2 = t.K + 2;
     const int j0 = blockIdx.x * T::TC, k = blockIdx.y, b = blockIdx.z;
@@ -274,11 +285,23 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
         const int m = i / (L / 4), l = i % (L / 4);
         cp_async8(mtab + i, m < 10 ? t.cosm + (size_t)m * L + l : t.sinm + (size_t)(m - 10) * L + l, 8);
     }
-    for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
-        const int c = i % T::TC, l = i / T::TC, j = j0 + c;
-        const bool ok = j < t.M;
-        cp_async8(A + l * T::RS + c, ok ? rho + (size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l) : rho,
-                  ok ? 8 : 0);
+    if (vec16) {
+        // 16-byte copies of the granules e = j0 .. j0+TC+1 of each row (RHO
+        // 16-byte aligned, JMAX+2 even); granules past the row read as zero
+        constexpr int NG = T::TC / 2 + 1;
+        for (int i = threadIdx.x; i < L * NG; i += blockDim.x) {
+            const int g = i % NG, l = i / NG, e = j0 + 2 * g;
+            const bool ok = e + 1 < J2;
+            cp_async16(A0 + l * T::RS + 2 * g, ok ? rho + (size_t)e + (size_t)J2 * ((k + 1) + (size_t)K2 * l) : rho,
+                       ok ? 16 : 0);
+        }
+    } else {
+        for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
+            const int c = i % T::TC, l = i / T::TC, j = j0 + c;
+            const bool ok = j < t.M;
+            cp_async8(A + l * T::RS + c, ok ? rho + (size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l) : rho,
+                      ok ? 8 : 0);
+        }
     }
     cp_async_wait_all();
     __syncthreads();
@@ -743,7 +766,10 @@ static cudaError_t forward_l(const DevTables &t, const BatchPtrs &bp, const Work
     const size_t sm = tile_bytes<L>() + (size_t)20 * (L / 4) * 8 + fft_table_bytes<L>();
     cudaError_t e = ensure_smem((const void *)k_forward<L>, sm);
     if (e != cudaSuccess) return e;
-    k_forward<L><<<dim3((t.M + T::TC - 1) / T::TC, t.NZ, nb), 256, sm, s>>>(t, bp, w);
+    // 16-byte row copies need every RHO 16-byte aligned and JMAX+2 even
+    int vec16 = (t.J + 2) % 2 == 0;
+    for (int i = 0; i < nb; ++i) vec16 = vec16 && reinterpret_cast<uintptr_t>(bp.rho[i]) % 16 == 0;
+    k_forward<L><<<dim3((t.M + T::TC - 1) / T::TC, t.NZ, nb), 256, sm, s>>>(t, bp, w, vec16);
     return cudaGetLastError();
 }
 
