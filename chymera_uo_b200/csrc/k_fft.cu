@@ -555,12 +555,25 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
 
     load_fft_tables(t.inv, fs);
     // A1(1..N+1) = modes 0..N, B1(2..N) = modes N+1..2N-1, B1(1) = B1(N+1) = 0
-    for (int i = threadIdx.x; i < (n + 1) * T::TC; i += blockDim.x) {
-        const int c = i % T::TC, q = i / T::TC, j = j0 + c;
-        const bool ok = j < t.J, okim = ok && q >= 1 && q < n;
-        const size_t col = (size_t)k * t.J + j, pl = (size_t)t.K * t.J;
-        cp_async8(A + (2 * q) * T::RS + c, ok ? X + (size_t)q * pl + col : X, ok ? 8 : 0);
-        cp_async8(A + (2 * q + 1) * T::RS + c, okim ? X + (size_t)(n + q) * pl + col : X, okim ? 8 : 0);
+    if ((t.J & 1) == 0) {
+        // JMAX even: 16-byte granules (columns j, j+1 both in range or both
+        // out), aligned since X, JMAX and j0 are
+        constexpr int NG = T::TC / 2;
+        for (int i = threadIdx.x; i < (n + 1) * NG; i += blockDim.x) {
+            const int g = i % NG, q = i / NG, j = j0 + 2 * g;
+            const bool ok = j < t.J, okim = ok && q >= 1 && q < n;
+            const size_t col = (size_t)k * t.J + j, pl = (size_t)t.K * t.J;
+            cp_async16(A + (2 * q) * T::RS + 2 * g, ok ? X + (size_t)q * pl + col : X, ok ? 16 : 0);
+            cp_async16(A + (2 * q + 1) * T::RS + 2 * g, okim ? X + (size_t)(n + q) * pl + col : X, okim ? 16 : 0);
+        }
+    } else {
+        for (int i = threadIdx.x; i < (n + 1) * T::TC; i += blockDim.x) {
+            const int c = i % T::TC, q = i / T::TC, j = j0 + c;
+            const bool ok = j < t.J, okim = ok && q >= 1 && q < n;
+            const size_t col = (size_t)k * t.J + j, pl = (size_t)t.K * t.J;
+            cp_async8(A + (2 * q) * T::RS + c, ok ? X + (size_t)q * pl + col : X, ok ? 8 : 0);
+            cp_async8(A + (2 * q + 1) * T::RS + c, okim ? X + (size_t)(n + q) * pl + col : X, okim ? 8 : 0);
+        }
     }
     cp_async_wait_all();
     __syncthreads();
