@@ -309,7 +309,14 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
     // azimuthal moments of each ring (pot/boundary.f:527-538), before DV, using
     // psi -> pi - psi, pi + psi, 2 pi - psi to fold the sum to a quarter period
     {
-        const int c = threadIdx.x / T::TPC, g = threadIdx.x % T::TPC;
+        // With 16 threads per column, lanes alternate between a warp's two
+        // columns (so that a half-warp reads 8 rows of 2 columns: no bank
+        // conflict at the even row stride); otherwise a column's threads are
+        // consecutive lanes.  SH is the lane distance between a column's
+        // threads g and g+1.
+        constexpr int SH = T::TPC == 16 ? 2 : 1;
+        const int c = SH == 2 ? 2 * (threadIdx.x >> 5) + (threadIdx.x & 1) : threadIdx.x / T::TPC;
+        const int g = SH == 2 ? (threadIdx.x & 31) >> 1 : threadIdx.x % T::TPC;
         constexpr int Q = L / 4;
         double acc[21];
 #pragma unroll
@@ -342,7 +349,7 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
             for (int i = 0; i < W / 2; ++i) {
                 const double send = up ? a[i] : a[W / 2 + i];
                 const double keep = up ? a[W / 2 + i] : a[i];
-                a[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                a[i] = keep + __shfl_xor_sync(0xffffffffu, send, o * SH);
             }
             base += up ? W / 2 : 0;
         }
