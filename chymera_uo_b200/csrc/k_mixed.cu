@@ -347,20 +347,24 @@ __device__ __forceinline__ void put_split(uint8_t *hi, uint8_t *lo, int row, int
 // FP16 hi/lo split of 32 consecutive B-tile rows c0..c0+31 (K index kq, the
 // caller's TMEM lane), values already scaled.  Lane pairs (2i, 2i+1) swap
 // halves so that each thread writes the (k even, k odd) pair of one row as a
-// half2: rows c0+u for even lanes, c0+u+1 for odd lanes.  Same roundings as
+// half2: rows c0+u for even lanes, c0+u+4 for odd lanes.  Same roundings as
 // put_split, element by element.
 __device__ __forceinline__ void split_rows32(uint8_t *hi, uint8_t *lo, const float *v, int c0, int kq, int lane,
                                              int R)
 {
     const int odd = lane & 1, ke = kq & ~1, kk = ke & 63, g = kk >> 3;
     const uint32_t base = (uint32_t)((ke >> 6) * (R * 128) + ((kk & 7) << 1));
+    // even lanes take rows u with u % 8 < 4, odd lanes rows u + 4: in the
+    // 128-byte swizzle the two rows' granules are disjoint, so the 32 lanes'
+    // stores fall on 32 distinct banks
 #pragma unroll
-    for (int u = 0; u < 32; u += 2) {
-        const float send = odd ? v[u] : v[u + 1];
+    for (int i = 0; i < 16; ++i) {
+        const int u = (i & 3) + ((i >> 2) << 3);
+        const float send = odd ? v[u] : v[u + 4];
         const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
         const float a = odd ? recv : v[u];        // K index ke
-        const float b = odd ? v[u + 1] : recv;    // K index ke + 1
-        const int row = c0 + u + odd;
+        const float b = odd ? v[u + 4] : recv;    // K index ke + 1
+        const int row = c0 + u + 4 * odd;
         const uint32_t off = base + (uint32_t)row * 128 + ((uint32_t)(g ^ (row & 7)) << 4);
         const __half2 h = __floats2half2_rn(a, b);
         const float2 hb = __half22float2(h);
