@@ -17,6 +17,8 @@
 // the recorded tables, staged in shared memory.
 #include "devplan.h"
 
+#include <type_traits>
+
 namespace chy {
 
 // ---------------------------------------------------------------------------
@@ -318,48 +320,62 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
         const int c = SH == 2 ? 2 * (threadIdx.x >> 5) + (threadIdx.x & 1) : threadIdx.x / T::TPC;
         const int g = SH == 2 ? (threadIdx.x & 31) >> 1 : threadIdx.x % T::TPC;
         constexpr int Q = L / 4;
-        double acc[21];
-#pragma unroll
-        for (int q = 0; q < 21; ++q) acc[q] = 0.0;
-        for (int l = g; l < Q; l += T::TPC) {
-            const double r1 = A[l * T::RS + c], r2 = A[(L / 2 - 1 - l) * T::RS + c];
-            const double r3 = A[(L / 2 + l) * T::RS + c], r4 = A[(L - 1 - l) * T::RS + c];
-            const double e = r1 + r4, f = r2 + r3, gg = r1 - r4, h = r3 - r2;
-            const double ce = e + f, co = e - f, se = gg + h, so = gg - h;
-            acc[0] += ce;
-#pragma unroll
-            for (int m = 1; m <= 10; ++m) {
-                acc[m] = __fma_rn(mtab[(m - 1) * Q + l], (m & 1) ? co : ce, acc[m]);
-                acc[10 + m] = __fma_rn(mtab[(9 + m) * Q + l], (m & 1) ? so : se, acc[10 + m]);
-            }
-        }
-        // Butterfly reduce-scatter over the column's TPC lanes (21 sums padded
-        // to 32): at each level a lane keeps half of its live sums and adds the
-        // partner's copy of them, so lane g ends with the column totals of
-        // sums base(g) .. base(g) + 32/TPC - 1, in a fixed order.
-        double a[32];
-#pragma unroll
-        for (int q = 0; q < 32; ++q) a[q] = q < 21 ? acc[q] : 0.0;
-        int base = 0;
-#pragma unroll
-        for (int lev = 0; (T::TPC >> (lev + 1)) >= 1; ++lev) {
-            const int o = T::TPC >> (lev + 1), W = 32 >> lev;
-            const bool up = (g & o) != 0;
-#pragma unroll
-            for (int i = 0; i < W / 2; ++i) {
-                const double send = up ? a[i] : a[W / 2 + i];
-                const double keep = up ? a[W / 2 + i] : a[i];
-                a[i] = keep + __shfl_xor_sync(0xffffffffu, send, o * SH);
-            }
-            base += up ? W / 2 : 0;
-        }
+        // The cosine sums (q = 0..10) and the sine sums (q = 11..20) are
+        // formed in two passes over the samples, so that only one set of
+        // accumulators is live at a time.  Butterfly reduce-scatter over the
+        // column's TPC lanes (the pass's sums padded to NS): at each level a
+        // lane keeps half of its live sums and adds the partner's copy of
+        // them, so lane g ends with the column totals of sums base(g) ..
+        // base(g) + NS/TPC - 1.  Every total is the same pairwise tree over
+        // the TPC lanes whichever lane ends with it, so the pass split
+        // changes no bit.
+        constexpr int NS = T::TPC > 16 ? T::TPC : 16;
         const int j = j0 + c;
-        if (j < t.M) {
-            double *mom = w.mom + (size_t)b * w.smom + (size_t)k * t.M + j;
+        double *mom = w.mom + (size_t)b * w.smom + (size_t)k * t.M + j;
+        auto pass = [&](auto sine) {
+            constexpr bool S = decltype(sine)::value;
+            constexpr int NQ = S ? 10 : 11, Q0 = S ? 11 : 0;
+            double a[NS];
 #pragma unroll
-            for (int i = 0; i < 32 / T::TPC; ++i)
-                if (base + i < 21) mom[(size_t)(base + i) * t.nring] = a[i];
-        }
+            for (int q = 0; q < NS; ++q) a[q] = 0.0;
+            for (int l = g; l < Q; l += T::TPC) {
+                const double r1 = A[l * T::RS + c], r2 = A[(L / 2 - 1 - l) * T::RS + c];
+                const double r3 = A[(L / 2 + l) * T::RS + c], r4 = A[(L - 1 - l) * T::RS + c];
+                if constexpr (!S) {
+                    const double e = r1 + r4, f = r2 + r3;
+                    const double ce = e + f, co = e - f;
+                    a[0] += ce;
+#pragma unroll
+                    for (int m = 1; m <= 10; ++m) a[m] = __fma_rn(mtab[(m - 1) * Q + l], (m & 1) ? co : ce, a[m]);
+                } else {
+                    const double gg = r1 - r4, h = r3 - r2;
+                    const double se = gg + h, so = gg - h;
+#pragma unroll
+                    for (int m = 1; m <= 10; ++m)
+                        a[m - 1] = __fma_rn(mtab[(9 + m) * Q + l], (m & 1) ? so : se, a[m - 1]);
+                }
+            }
+            int base = 0;
+#pragma unroll
+            for (int lev = 0; (T::TPC >> (lev + 1)) >= 1; ++lev) {
+                const int o = T::TPC >> (lev + 1), W = NS >> lev;
+                const bool up = (g & o) != 0;
+#pragma unroll
+                for (int i = 0; i < W / 2; ++i) {
+                    const double send = up ? a[i] : a[W / 2 + i];
+                    const double keep = up ? a[W / 2 + i] : a[i];
+                    a[i] = keep + __shfl_xor_sync(0xffffffffu, send, o * SH);
+                }
+                base += up ? W / 2 : 0;
+            }
+            if (j < t.M) {
+#pragma unroll
+                for (int i = 0; i < NS / T::TPC; ++i)
+                    if (base + i < NQ) mom[(size_t)(Q0 + base + i) * t.nring] = a[i];
+            }
+        };
+        pass(std::integral_constant<bool, false>{});
+        pass(std::integral_constant<bool, true>{});
     }
     __syncthreads();
 
