@@ -74,7 +74,8 @@ __host__ __device__ inline uint32_t kmaj_off(int r, int k, int R)
 struct MixedDev {
     const uint8_t *aimg;        // [U hi, U lo, V hi, V lo] swizzled tiles (2^12 scaled)
     const float *lam;           // [128]
-    const float2 *sweep;        // [N+1][ntile][128] {e or f, 1/D} of the radial sweeps
+    const float *sw_mul;        // [N+1][ntile][128] multipliers e or f of the radial sweeps
+    const float *sw_piv;        // [N+1][ntile][128] pivot reciprocals 1/D
     double *xbuf;               // [nb][L][K][J] FP64 iterate
     size_t sxb;
     double *corr;               // [nb][L][8][2] per mode: sum delta^2, sum x^2
@@ -440,7 +441,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     uint64_t *bar_mma = reinterpret_cast<uint64_t *>(f_edge + 512);
     uint64_t *bar_a = bar_mma + 1;
     uint64_t *bar_ring = bar_a + 1;   // [kRingSlots] residual ring slots
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_ring + kRingSlots);
+    uint64_t *bar_cv = bar_ring + kRingSlots;   // sweep multipliers copied in
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_cv + 1);
     int *s_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
     // ---- setup: tensor memory (all 512 columns), barriers, m-independent tables
@@ -452,6 +454,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
         mbar_init(bar_mma, 1);
         mbar_init(bar_a, 1);
         for (int i = 0; i < kRingSlots; ++i) mbar_init(bar_ring + i, 1);
+        mbar_init(bar_cv, 1);
         *s_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -479,6 +482,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     const int nit = kRes ? min(x.nit, 2) : x.nit;
     uint32_t ph_mma = 0, ph_a = 0;
     uint32_t ring_ph = 0, ring_pend = 0;   // residual ring slots: phase parity, copies in flight
+    uint32_t ph_cv = 0;
+    bool cv_pend = false;
     bool failed = false;
 
     const long long items = (long long)nb * t.L;
@@ -818,67 +823,86 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             if (a_inflight && !wait_all(bar_a, ph_a)) { failed = true; break; }
             a_inflight = false;
             if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma);
+            // the first chunk of pivot reciprocals is loaded while the product runs
+            const float *swp = x.sw_piv + (size_t)m * NT * 128 + kq;   // row j at swp[j * 128]
+            const int h = 32 * ((M + 63) / 64);   // M >= 63, h < M, h % 32 == 0
+            const int cl = ((M - 1) / 32) * 32;   // the bottom-up sweep's first chunk
+            float R[32];
+#pragma unroll
+            for (int u = 0; u < 32; ++u) R[u] = swp[(size_t)((jh == 0 ? 0 : cl) + u) * 128];
             if (!wait_all(bar_mma, ph_mma)) { failed = true; break; }
             tc_fence_after();
-            if (tid == 0) {   // A tile free: bring in V
+            float *cvs = reinterpret_cast<float *>(sBh);   // [j][p] multipliers for the back sweeps
+            if (tid == 0) {
+                // B tile free: this m's multipliers for the back sweeps, then
+                // the A tile: V
+                const float *src = x.sw_mul + (size_t)m * NT * 128;
+                mbar_expect_tx(bar_cv, (uint32_t)NT * 512);
+                for (int q = 0; q < 4; ++q) bulk_g2s(cvs + q * NT * 32, src + q * NT * 32, (uint32_t)NT * 128, bar_cv);
                 mbar_expect_tx(bar_a, kAImg);
                 bulk_g2s(sA, x.aimg + kAImg, kAImg, bar_a);
             }
+            cv_pend = true;
             a_inflight = true;
             // ---- radial sweeps (T_r(m) + lam_p) w = W_p, top-down over rows
             // [0, h) and bottom-up over [h, M), meeting in the middle.  The
             // multipliers and pivot reciprocals come from the sweep table, so
-            // each row costs one dependent FMA; the table loads of a chunk are
-            // independent of the recurrence and issue ahead of it.
+            // each row costs one dependent FMA.  The elimination reads the
+            // pivot reciprocals from global memory one 32-row chunk ahead of
+            // the recurrence; the multipliers, which only the back sweeps
+            // need, arrive in shared memory as one bulk copy meanwhile.
             float xmax = 0.0f;
             {
                 const int p = kq;
                 const bool live = p < NZ;
-                const int h = 32 * ((M + 63) / 64);   // M >= 63, h < M, h % 32 == 0
                 const uint32_t tb = tmem + lane_base + acc;
-                const float2 *sw = x.sweep + (size_t)m * NT * 128 + p;   // row j at sw[j * 128]
-                float *cvs = reinterpret_cast<float *>(sBh);   // [j][p] multipliers for the back sweeps
                 float yv[32];
-                float2 T[32];
+                float Rn[32];
                 if (jh == 0) {
                     float yp = 0.f;
                     for (int c0 = 0; c0 < h; c0 += 32) {
+                        if (c0 + 32 < h) {
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) T[u] = sw[(size_t)(c0 + u) * 128];
+                            for (int u = 0; u < 32; ++u) Rn[u] = swp[(size_t)(c0 + 32 + u) * 128];
+                        }
                         tm_ld32(tb + c0, yv);
 #pragma unroll
                         for (int u = 0; u < 32; ++u) {
-                            const float rr = T[u].y, ar = f_t[c0 + u].y * rr;
+                            const float rr = R[u], ar = f_t[c0 + u].y * rr;
                             yp = fmaf(-ar, yp, yv[u] * rr);
                             yv[u] = yp;
                         }
                         tm_st32_nw(tb + c0, yv);
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) cvs[(c0 + u) * 128 + p] = T[u].x;
+                        for (int u = 0; u < 32; ++u) R[u] = Rn[u];
                     }
                     f_xch[p * 4 + 0] = yp;
                 } else {
                     float yp = 0.f;
-                    const int cl = ((M - 1) / 32) * 32;
                     for (int c0 = cl; c0 >= h; c0 -= 32) {
+                        if (c0 - 32 >= h) {
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) T[u] = sw[(size_t)(c0 + u) * 128];
+                            for (int u = 0; u < 32; ++u) Rn[u] = swp[(size_t)(c0 - 32 + u) * 128];
+                        }
                         tm_ld32(tb + c0, yv);
 #pragma unroll
                         for (int u = 31; u >= 0; --u) {
-                            const float rr = T[u].y, cr = f_t[c0 + u].z * rr;
+                            const float rr = R[u], cr = f_t[c0 + u].z * rr;
                             const float yn = fmaf(-cr, yp, yv[u] * rr);
                             yp = (c0 + u < M) ? yn : yp;   // uniform
                             yv[u] = yn;
                         }
                         tm_st32_nw(tb + c0, yv);
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) cvs[(c0 + u) * 128 + p] = T[u].x;
+                        for (int u = 0; u < 32; ++u) R[u] = Rn[u];
                     }
                     f_xch[p * 4 + 2] = yp;
                 }
                 tm_wait_st();
-                __syncthreads();
+                // the multipliers have landed (the barrier inside)
+                const bool cv_ok = wait_all(bar_cv, ph_cv);
+                cv_pend = false;
+                if (!cv_ok) { failed = true; break; }
                 // meeting rows h-1 (top) and h (bottom):
                 // x_t = y'_t + (1-e_t) x_u, x_u = y''_u + (1-f_u) x_t
                 float xt, xu;
@@ -892,11 +916,11 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     float xn = xt;   // x_{j+1} while sweeping up
                     for (int c0 = h - 32; c0 >= 0; c0 -= 32) {
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) T[u].x = cvs[(c0 + u) * 128 + p];
+                        for (int u = 0; u < 32; ++u) Rn[u] = cvs[(c0 + u) * 128 + p];
                         tm_ld32(tb + c0, yv);
 #pragma unroll
                         for (int u = 31; u >= 0; --u) {
-                            float xv = yv[u] + (1.0f - T[u].x) * xn;
+                            float xv = yv[u] + (1.0f - Rn[u]) * xn;
                             xv = (c0 + u == h - 1) ? xt : xv;
                             xn = xv;
                             yv[u] = live ? xv : 0.f;
@@ -908,11 +932,11 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     float xp = xu;   // x_{j-1} while sweeping down
                     for (int c0 = h; c0 < NT; c0 += 32) {
 #pragma unroll
-                        for (int u = 0; u < 32; ++u) T[u].x = cvs[(c0 + u) * 128 + p];
+                        for (int u = 0; u < 32; ++u) Rn[u] = cvs[(c0 + u) * 128 + p];
                         tm_ld32(tb + c0, yv);
 #pragma unroll
                         for (int u = 0; u < 32; ++u) {
-                            float xv = yv[u] + (1.0f - T[u].x) * xp;
+                            float xv = yv[u] + (1.0f - Rn[u]) * xp;
                             xv = (c0 + u == h) ? xu : xv;
                             xp = xv;
                             yv[u] = (live && c0 + u < M) ? xv : 0.f;
@@ -1079,6 +1103,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     if (a_inflight && !failed) mbar_wait(bar_a, ph_a);
     for (int sl = 0; sl < kRingSlots; ++sl)
         if (ring_pend & (1u << sl)) mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u);
+    if (cv_pend) mbar_wait(bar_cv, ph_cv);
     if (failed && tid == 0) atomicExch(x.err, 1);
     tc_fence_before();
     __syncthreads();
@@ -1098,14 +1123,16 @@ bool chy_mixed_supported(const chy::HostPlan *hp)
 // Radial sweep table: for every azimuthal index m = 0..N and vertical
 // eigenvalue p (padding rows use -1), the multipliers of the two-sided
 // elimination of (T_r(m) + lam_p) in excess form and the pivot reciprocals,
-// {e_j or f_j, 1/D_j} as FP32 pairs, layout [m][j][p] (j < ntile, p < 128).
+// as two FP32 planes, the multipliers e_j or f_j, then the pivot reciprocals
+// 1/D_j, each of layout [m][j][p] (j < ntile, p < 128).
 // Rows [0, h) are eliminated top-down, rows [h, M) bottom-up,
 // h = 32 ceil(M / 64).  They do not depend on the data, so they are formed
 // once, in FP64, here.
 static std::vector<float> sweep_table(const chy::HostPlan &hp)
 {
     const int M = hp.M, NT = round64(hp.J), n = hp.N, h = 32 * ((M + 63) / 64);
-    std::vector<float> t((size_t)(n + 1) * NT * 128 * 2, 0.0f);
+    const size_t plane = (size_t)(n + 1) * NT * 128;
+    std::vector<float> t(plane * 2, 0.0f);
     std::vector<double> g(M);
     for (int m = 0; m <= n; ++m) {
         const double xl2 = 2.0 * (hp.xlamm[m] - 1.0);
@@ -1118,9 +1145,9 @@ static std::vector<float> sweep_table(const chy::HostPlan &hp)
         for (int p = 0; p < 128; ++p) {
             const double lam = p < hp.NZ ? hp.lam[p] : -1.0;
             auto put = [&](int j, double c, double r) {
-                float *q = &t[(((size_t)m * NT + j) * 128 + p) * 2];
-                q[0] = (float)c;
-                q[1] = (float)r;
+                const size_t o = ((size_t)m * NT + j) * 128 + p;
+                t[o] = (float)c;
+                t[plane + o] = (float)r;
             };
             double e = 0.0;
             for (int j = 0; j < h; ++j) {
@@ -1184,7 +1211,8 @@ void chy_mixed_bind_tables(chy_plan *p, char *dev_base)
     size_t lam_off = (((size_t)(dev_base - p->d_tables) + 2 * kAImg) + 255) & ~(size_t)255;
     p->mx->dev.lam = reinterpret_cast<const float *>(p->d_tables + lam_off);
     const size_t sw_off = (lam_off + 128 * sizeof(float) + 255) & ~(size_t)255;
-    p->mx->dev.sweep = reinterpret_cast<const float2 *>(p->d_tables + sw_off);
+    p->mx->dev.sw_mul = reinterpret_cast<const float *>(p->d_tables + sw_off);
+    p->mx->dev.sw_piv = p->mx->dev.sw_mul + (size_t)(p->hp.N + 1) * round64(p->hp.J) * 128;
 }
 
 // Per-mode correction sums and the error word; the FP64 iterate of the
