@@ -17,6 +17,9 @@
 // the recorded tables, staged in shared memory.
 #include "devplan.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <type_traits>
 
 namespace chy {
@@ -69,6 +72,36 @@ struct FftSmem {
     int *perm;         // [n]
     double *rt;        // [nh][2]
 };
+
+// 3-D tensor maps over each solve's RHO(J+2, K+2, L), one per batch slot:
+// boxes of TC+2 columns x one K x up to 256 L, no swizzle, no multicast.  A
+// box lands as L rows of TC+2 doubles, the tile's own row stride.
+struct RhoMaps {
+    CUtensorMap m[kMaxBatchPtrs];
+};
+
+__device__ __forceinline__ uint32_t sm32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            sm32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(sm32(bar))
+        : "memory");
+}
+// bounded wait on an mbarrier phase; false on timeout
+__device__ __forceinline__ bool fwd_bar_wait(uint64_t *bar, uint32_t parity)
+{
+    for (long long i = 0; i < (1ll << 26); ++i) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(sm32(bar)), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
 
 // Asynchronous global -> shared copies (bytes = 0: the destination is zeroed;
 // src must still be a valid address).  cp_async_wait_all() then a barrier
@@ -265,10 +298,11 @@ __device__ __forceinline__ void realtr_pairs(double *A, const FftSmem &s)
 // POT3 copies into PHI (pot/pot3.f:70-82) and BDYGEN integrates
 // (pot/boundary.f:366-370) -- and writes X interior plus MOM.
 template <int L>
-__global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work w, int vec16)
+__global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work w, int vec16,
+                                                 const __grid_constant__ RhoMaps maps)
 {
     using T = Tile<L>;
-    extern __shared__ __align__(16) char smem_raw[];
+    extern __shared__ __align__(128) char smem_raw[];
     // Row l of the tile holds RHO(J0+1 .. J0+TC+2, K, L) at columns -1 .. TC:
     // the view A is shifted by one element, so A[l*RS + c] is column
     // j = j0 + c (RHO(j + 2, ...)), and the 16-byte granules of a row start
@@ -280,6 +314,22 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
     const int J2 = t.J + 2, K2 = t.K + 2;
     const int j0 = blockIdx.x * T::TC, k = blockIdx.y, b = blockIdx.z;
     const double *rho = bp.rho[b];
+    // vec16 == 2: the tile arrives as TMA boxes of the tensor map of this
+    // solve's RHO, counted on tbar (after the tables)
+    uint64_t *tbar = reinterpret_cast<uint64_t *>(smem_raw + (size_t)T::ROWS * T::RS * 8 + (size_t)20 * (L / 4) * 8 +
+                                                  fft_table_bytes<L>());
+    if (vec16 == 2) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm32(tbar)));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm32(tbar)),
+                         "r"((uint32_t)(L * T::RS * 8)));
+            for (int l0 = 0; l0 < L; l0 += 256) tma_load_3d(A0 + (size_t)l0 * T::RS, &maps.m[b], j0, k + 1, l0, tbar);
+        }
+    }
 
     // tables and the tile's samples: every copy in flight at once
     load_fft_tables(t.fwd, fs);
@@ -287,7 +337,9 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
         const int m = i / (L / 4), l = i % (L / 4);
         cp_async8(mtab + i, m < 10 ? t.cosm + (size_t)m * L + l : t.sinm + (size_t)(m - 10) * L + l, 8);
     }
-    if (vec16) {
+    if (vec16 == 2) {
+        // copies issued above
+    } else if (vec16) {
         // 16-byte copies of the granules e = j0 .. j0+TC+1 of each row (RHO
         // 16-byte aligned, JMAX+2 even); granules past the row read as zero
         constexpr int NG = T::TC / 2 + 1;
@@ -306,6 +358,9 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
         }
     }
     cp_async_wait_all();
+    // a tile that did not arrive in time makes this tile's modes NaN, so the
+    // failure reaches PHI instead of passing silently
+    const bool landed = vec16 != 2 || fwd_bar_wait(tbar, 0);
     __syncthreads();
 
     // azimuthal moments of each ring (pot/boundary.f:527-538), before DV, using
@@ -403,6 +458,7 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
             if (jp != kp) xc[(size_t)kp * pl] = (aa - re) * t.sf1;
             if (jp >= 1) xc[(size_t)(n + jp) * pl] = (im + bb) * t.sf1;
             if (jp >= 1 && jp != kp) xc[(size_t)(n + kp) * pl] = (im - bb) * t.sf1;
+            if (!landed) xc[0] = __longlong_as_double(0x7ff8000000000000ll);
         }
     }
 }
@@ -795,17 +851,48 @@ __global__ void k_diag(DevTables t, Work w)
 template <int L>
 static size_t tile_bytes() { return (size_t)Tile<L>::ROWS * Tile<L>::RS * sizeof(double); }
 
+// cuTensorMapEncodeTiled from the driver, through the runtime
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        cudaGetLastError();
+        return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+    }();
+    return fn;
+}
+
 template <int L>
 static cudaError_t forward_l(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s)
 {
     using T = Tile<L>;
-    const size_t sm = tile_bytes<L>() + (size_t)20 * (L / 4) * 8 + fft_table_bytes<L>();
+    const size_t sm = tile_bytes<L>() + (size_t)20 * (L / 4) * 8 + fft_table_bytes<L>() + 16;
     cudaError_t e = ensure_smem((const void *)k_forward<L>, sm);
     if (e != cudaSuccess) return e;
     // 16-byte row copies need every RHO 16-byte aligned and JMAX+2 even
     int vec16 = (t.J + 2) % 2 == 0;
     for (int i = 0; i < nb; ++i) vec16 = vec16 && reinterpret_cast<uintptr_t>(bp.rho[i]) % 16 == 0;
-    k_forward<L><<<dim3((t.M + T::TC - 1) / T::TC, t.NZ, nb), 256, sm, s>>>(t, bp, w, vec16);
+    // with 16-byte aligned rows, the tiles come through one tensor map per
+    // solve (encoded here: host arithmetic only, passed by value)
+    RhoMaps maps;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (vec16 && enc) {
+        bool ok = true;
+        for (int i = 0; i < nb && ok; ++i) {
+            const cuuint64_t dims[3] = {(cuuint64_t)(t.J + 2), (cuuint64_t)(t.K + 2), (cuuint64_t)L};
+            const cuuint64_t strides[2] = {(cuuint64_t)(t.J + 2) * 8, (cuuint64_t)(t.J + 2) * (t.K + 2) * 8};
+            const cuuint32_t box[3] = {(cuuint32_t)T::RS, 1u, (cuuint32_t)(L < 256 ? L : 256)}, es[3] = {1, 1, 1};
+            ok = enc(&maps.m[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(bp.rho[i]), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        }
+        if (ok) vec16 = 2;
+    }
+    k_forward<L><<<dim3((t.M + T::TC - 1) / T::TC, t.NZ, nb), 256, sm, s>>>(t, bp, w, vec16, maps);
     return cudaGetLastError();
 }
 
