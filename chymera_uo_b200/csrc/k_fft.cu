@@ -20,6 +20,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstring>
 #include <type_traits>
 
 namespace chy {
@@ -63,6 +64,10 @@ struct Tile {
     static constexpr int RS = TC + 2;                               // row stride (doubles, even)
     static constexpr int ROWS = L + 2;
     static constexpr int TPC = 256 / TC;                            // threads per column
+    // inverse tile (split layout, row stride TC): Re rows 0..N, Im rows from
+    // IM0 (a 128-byte boundary, for the tensor-map copies)
+    static constexpr int IM0 = (TC * 8) % 128 == 0 ? N + 1 : N + 2;
+    static constexpr int ROWSI = IM0 + N + 1;
 };
 
 // Shared-memory copy of one direction's tables.
@@ -210,11 +215,16 @@ __device__ __forceinline__ void butterfly(double &a0, double &b0, double &a1, do
 // stages: a thread loads them, applies stage S's R_{S+1} butterflies and then
 // stage S+1's R_S butterflies in registers, and stores them back.  Each
 // butterfly is the one the element-by-element stage loop would apply.
-template <int L, int S, bool FWD>
+//
+// Layout of the complex element e in the tile (row stride RS): interleaved
+// (Re in row 2e, Im in row 2e+1) or split (Re in row e, Im in row IM0+e).
+template <int L, int S, bool FWD, int RS = Tile<L>::RS, bool SPLIT = false>
 __device__ __forceinline__ void stage_pairs(double *A, const FftSmem &s, const FftDev &f)
 {
     using T = Tile<L>;
     using Sh = Shape<T::N>;
+    auto rre = [](int e) { return SPLIT ? e : 2 * e; };
+    auto rim = [](int e) { return SPLIT ? T::IM0 + e : 2 * e + 1; };
     if constexpr (S < Sh::nst()) {
         constexpr bool two = S + 1 < Sh::nst();
         constexpr int R1 = Sh::radix(S), H1 = Sh::span(S);
@@ -227,8 +237,8 @@ __device__ __forceinline__ void stage_pairs(double *A, const FftSmem &s, const F
             double re[G], im[G];
 #pragma unroll
             for (int i = 0; i < G; ++i) {
-                re[i] = A[(2 * (base + i * H2)) * T::RS + c];
-                im[i] = A[(2 * (base + i * H2) + 1) * T::RS + c];
+                re[i] = A[rre(base + i * H2) * RS + c];
+                im[i] = A[rim(base + i * H2) * RS + c];
             }
             // stage S: butterflies m = 0..R2-1 on elements m + t R2 (t < R1)
 #pragma unroll
@@ -258,35 +268,36 @@ __device__ __forceinline__ void stage_pairs(double *A, const FftSmem &s, const F
             }
 #pragma unroll
             for (int i = 0; i < G; ++i) {
-                A[(2 * (base + i * H2)) * T::RS + c] = re[i];
-                A[(2 * (base + i * H2) + 1) * T::RS + c] = im[i];
+                A[rre(base + i * H2) * RS + c] = re[i];
+                A[rim(base + i * H2) * RS + c] = im[i];
             }
         }
         __syncthreads();
-        stage_pairs<L, two ? S + 2 : S + 1, FWD>(A, s, f);
+        stage_pairs<L, two ? S + 2 : S + 1, FWD, RS, SPLIT>(A, s, f);
     }
 }
 
 // REALTR (pot/fft.f:2-70): the N/2+1 (j, N-j) pairs are independent once the
-// recurrence values are tabulated.
+// recurrence values are tabulated.  On the inverse tile: split layout, row
+// stride TC (Re of element e in row e, Im in row IM0+e).
 template <int L>
 __device__ __forceinline__ void realtr_pairs(double *A, const FftSmem &s)
 {
     using T = Tile<L>;
-    constexpr int n = T::N, nh = n / 2 + 1;
+    constexpr int n = T::N, nh = n / 2 + 1, RS = T::TC, I0 = T::IM0;
     for (int w = threadIdx.x; w < nh * T::TC; w += blockDim.x) {
         const int c = w % T::TC, j = w / T::TC, k = n - j;
         const double cn = s.rt[2 * j], sn = s.rt[2 * j + 1];
-        const double aj = A[(2 * j) * T::RS + c], bj = A[(2 * j + 1) * T::RS + c];
-        const double ak = A[(2 * k) * T::RS + c], bk = A[(2 * k + 1) * T::RS + c];
+        const double aj = A[j * RS + c], bj = A[(I0 + j) * RS + c];
+        const double ak = A[k * RS + c], bk = A[(I0 + k) * RS + c];
         const double aa = aj + ak, ab = aj - ak, ba = bj + bk, bb = bj - bk;
         const double re = cn * ba + sn * ab, im = sn * ba - cn * ab;
         if (j != k) {
-            A[(2 * k + 1) * T::RS + c] = im - bb;
-            A[(2 * k) * T::RS + c] = aa - re;
+            A[(I0 + k) * RS + c] = im - bb;
+            A[k * RS + c] = aa - re;
         }
-        A[(2 * j + 1) * T::RS + c] = im + bb;
-        A[(2 * j) * T::RS + c] = aa + re;
+        A[(I0 + j) * RS + c] = im + bb;
+        A[j * RS + c] = aa + re;
     }
     __syncthreads();
 }
@@ -619,22 +630,48 @@ __device__ __forceinline__ void star_pos(const StarDev &x, const Work &w, int b,
 }
 
 template <int L>
-__global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work w, StarDev x)
+__global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work w, StarDev x, int xmode,
+                                                 const __grid_constant__ CUtensorMap xmap)
 {
     using T = Tile<L>;
-    constexpr int n = T::N;
-    extern __shared__ __align__(16) char smem_raw[];
+    constexpr int n = T::N, RS = T::TC, I0 = T::IM0;
+    extern __shared__ __align__(128) char smem_raw[];
+    // Split layout, row stride TC: row q holds A1(q+1) = mode q (q = 0..N),
+    // row IM0+q holds B1(q+1) = mode N+q (q = 1..N-1); B1(1) = B1(N+1) = 0.
     double *A = (double *)smem_raw;
-    double *red = A + (size_t)T::ROWS * T::RS;   // [L/2] ZAXPHI values
+    double *red = A + (size_t)T::ROWSI * RS;   // [L/2] ZAXPHI values
     FftSmem fs = carve_fft<L>((char *)(red + L / 2));
+    uint64_t *tbar = reinterpret_cast<uint64_t *>(smem_raw + (size_t)T::ROWSI * RS * 8 + (size_t)(L / 2) * 8 +
+                                                  fft_table_bytes<L>());
     const int J2 = t.J + 2, K2 = t.K + 2;
     const int j0 = blockIdx.x * T::TC, k = blockIdx.y, b = blockIdx.z;
     const double *X = w.X + (size_t)b * w.sX;
     double *phi = bp.phi[b];
 
+    // xmode 2: two sets of TMA boxes of the tensor map over X (J, K, L x batch),
+    // TC columns x one K x up to 256 modes: modes 0..N-1 into rows 0..N-1 and
+    // modes N..2N-1 into rows IM0..IM0+N-1; mode N then moves to row N and rows
+    // IM0 and IM0+N become B1(1) = B1(N+1) = 0
+    if (xmode == 2) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sm32(tbar)));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            constexpr int B = n < 256 ? n : 256;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm32(tbar)),
+                         "r"((uint32_t)(2 * n * RS * 8)));
+            for (int z0 = 0; z0 < n; z0 += B) {
+                tma_load_3d(A + (size_t)z0 * RS, &xmap, j0, k, b * L + z0, tbar);
+                tma_load_3d(A + (size_t)(I0 + z0) * RS, &xmap, j0, k, b * L + n + z0, tbar);
+            }
+        }
+    }
     load_fft_tables(t.inv, fs);
-    // A1(1..N+1) = modes 0..N, B1(2..N) = modes N+1..2N-1, B1(1) = B1(N+1) = 0
-    if ((t.J & 1) == 0) {
+    if (xmode == 2) {
+        // copies issued above
+    } else if (xmode == 1) {
         // JMAX even: 16-byte granules (columns j, j+1 both in range or both
         // out), aligned since X, JMAX and j0 are
         constexpr int NG = T::TC / 2;
@@ -642,27 +679,39 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
             const int g = i % NG, q = i / NG, j = j0 + 2 * g;
             const bool ok = j < t.J, okim = ok && q >= 1 && q < n;
             const size_t col = (size_t)k * t.J + j, pl = (size_t)t.K * t.J;
-            cp_async16(A + (2 * q) * T::RS + 2 * g, ok ? X + (size_t)q * pl + col : X, ok ? 16 : 0);
-            cp_async16(A + (2 * q + 1) * T::RS + 2 * g, okim ? X + (size_t)(n + q) * pl + col : X, okim ? 16 : 0);
+            cp_async16(A + q * RS + 2 * g, ok ? X + (size_t)q * pl + col : X, ok ? 16 : 0);
+            cp_async16(A + (I0 + q) * RS + 2 * g, okim ? X + (size_t)(n + q) * pl + col : X, okim ? 16 : 0);
         }
     } else {
         for (int i = threadIdx.x; i < (n + 1) * T::TC; i += blockDim.x) {
             const int c = i % T::TC, q = i / T::TC, j = j0 + c;
             const bool ok = j < t.J, okim = ok && q >= 1 && q < n;
             const size_t col = (size_t)k * t.J + j, pl = (size_t)t.K * t.J;
-            cp_async8(A + (2 * q) * T::RS + c, ok ? X + (size_t)q * pl + col : X, ok ? 8 : 0);
-            cp_async8(A + (2 * q + 1) * T::RS + c, okim ? X + (size_t)(n + q) * pl + col : X, okim ? 8 : 0);
+            cp_async8(A + q * RS + c, ok ? X + (size_t)q * pl + col : X, ok ? 8 : 0);
+            cp_async8(A + (I0 + q) * RS + c, okim ? X + (size_t)(n + q) * pl + col : X, okim ? 8 : 0);
         }
     }
     cp_async_wait_all();
+    // a tile that did not arrive in time makes this tile's PHI NaN, so the
+    // failure shows instead of passing silently
+    const bool landed = xmode != 2 || fwd_bar_wait(tbar, 0);
     __syncthreads();
+    if (xmode == 2) {
+        if (threadIdx.x < T::TC) {
+            const int c = threadIdx.x;
+            A[n * RS + c] = landed ? A[I0 * RS + c] : __longlong_as_double(0x7ff8000000000000ll);
+            A[I0 * RS + c] = 0.0;
+            A[(I0 + n) * RS + c] = 0.0;
+        }
+        __syncthreads();
+    }
     realtr_pairs<L>(A, fs);
-    stage_pairs<L, 0, false>(A, fs, t.inv);
+    stage_pairs<L, 0, false, T::TC, true>(A, fs, t.inv);
 
     // sample l of column c in natural order, times SF2 = 0.5 (pot/pot3.f:276-279)
     auto sample = [&](int l, int c) -> double {
         const int src = fs.perm[l >> 1];
-        return 0.5 * A[(2 * src + (l & 1)) * T::RS + c];
+        return 0.5 * A[((l & 1) ? I0 + src : src) * RS + c];
     };
     // PHI = PHI + STARPHI after POT3 (pot/ExternalPot.f:50), fused into the
     // stores: v is POT3's value of the cell (jj, kk, l)
@@ -901,10 +950,25 @@ static cudaError_t inverse_l(const DevTables &t, const BatchPtrs &bp, const Work
                              cudaStream_t s, int *launches)
 {
     using T = Tile<L>;
-    const size_t sm = tile_bytes<L>() + (size_t)(L / 2) * 8 + fft_table_bytes<L>();
+    const size_t sm = (size_t)T::ROWSI * T::TC * sizeof(double) + (size_t)(L / 2) * 8 + fft_table_bytes<L>() + 16;
     cudaError_t e = ensure_smem((const void *)k_inverse<L>, sm);
     if (e != cudaSuccess) return e;
-    k_inverse<L><<<dim3((t.J + T::TC - 1) / T::TC, t.K, nb), 256, sm, s>>>(t, bp, w, x);
+    // X rows through a tensor map when JMAX is even (16-byte strides), else
+    // 8-byte copies
+    int xmode = (t.J & 1) == 0 ? 1 : 0;
+    CUtensorMap xmap;
+    std::memset(&xmap, 0, sizeof xmap);
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (xmode == 1 && enc && reinterpret_cast<uintptr_t>(w.X) % 16 == 0) {
+        const cuuint64_t dims[3] = {(cuuint64_t)t.J, (cuuint64_t)t.K, (cuuint64_t)L * nb};
+        const cuuint64_t strides[2] = {(cuuint64_t)t.J * 8, (cuuint64_t)t.J * t.K * 8};
+        const cuuint32_t box[3] = {(cuuint32_t)T::TC, 1u, (cuuint32_t)(T::N < 256 ? T::N : 256)}, es[3] = {1, 1, 1};
+        if (enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, w.X, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+            xmode = 2;
+    }
+    k_inverse<L><<<dim3((t.J + T::TC - 1) / T::TC, t.K, nb), 256, sm, s>>>(t, bp, w, x, xmode, xmap);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     *launches = 2;
     if (x.on) {
