@@ -404,7 +404,9 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
             double a[NS];
 #pragma unroll
             for (int q = 0; q < NS; ++q) a[q] = 0.0;
-            for (int l = g; l < Q; l += T::TPC) {
+#pragma unroll
+            for (int il = 0; il < Q / T::TPC; ++il) {
+                const int l = g + il * T::TPC;
                 const double r1 = A[l * T::RS + c], r2 = A[(L / 2 - 1 - l) * T::RS + c];
                 const double r3 = A[(L / 2 + l) * T::RS + c], r4 = A[(L - 1 - l) * T::RS + c];
                 if constexpr (!S) {
@@ -720,13 +722,21 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
     auto out = [&](int jj, int kk, int l, double v) -> double {
         return x.on ? __dadd_rn(v, star_phi(t, x, ix, iy, jj, kk, l)) : v;
     };
-    for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) {
+    auto store = [&](int i) {
         const int c = i % T::TC, l = i / T::TC, j = j0 + c;
         if (j < t.J) {
             const double v = sample(l, c);
             phi[(size_t)(j + 1) + (size_t)J2 * ((k + 1) + (size_t)K2 * l)] = out(j + 1, k + 1, l, v);
             if (k == 0) phi[(size_t)(j + 1) + (size_t)J2 * ((size_t)K2 * l)] = out(j + 1, 0, l, v);   // PHI(J,1,L)
         }
+    };
+    if (x.on) {
+        for (int i = threadIdx.x; i < L * T::TC; i += blockDim.x) store(i);
+    } else {
+        // 256 threads: a compile-time trip count, so that the shared-memory
+        // reads of several cells issue together
+#pragma unroll 4
+        for (int it = 0; it < L * T::TC / 256; ++it) store(threadIdx.x + 256 * it);
     }
     if (j0 == 0) {
         for (int l = threadIdx.x; l < L; l += blockDim.x) {
