@@ -285,7 +285,10 @@ __device__ __forceinline__ void realtr_pairs(double *A, const FftSmem &s)
 {
     using T = Tile<L>;
     constexpr int n = T::N, nh = n / 2 + 1, RS = T::TC, I0 = T::IM0;
-    for (int w = threadIdx.x; w < nh * T::TC; w += blockDim.x) {
+#pragma unroll
+    for (int it = 0; it < (nh * T::TC + 255) / 256; ++it) {
+        const int w = threadIdx.x + 256 * it;
+        if (w >= nh * T::TC) break;
         const int c = w % T::TC, j = w / T::TC, k = n - j;
         const double cn = s.rt[2 * j], sn = s.rt[2 * j + 1];
         const double aj = A[j * RS + c], bj = A[(I0 + j) * RS + c];
@@ -457,7 +460,10 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
     double *X = w.X + (size_t)b * w.sX;
     constexpr int n = T::N, nh = n / 2 + 1;
     const size_t pl = (size_t)t.K * t.J;
-    for (int i = threadIdx.x; i < nh * T::TC; i += blockDim.x) {
+#pragma unroll
+    for (int it = 0; it < (nh * T::TC + 255) / 256; ++it) {
+        const int i = threadIdx.x + 256 * it;
+        if (i >= nh * T::TC) break;
         const int c = i % T::TC, jp = i / T::TC, kp = n - jp, j = j0 + c;
         const int sj = fs.perm[jp], sk = fs.perm[kp < n ? kp : 0];
         const double cn = fs.rt[2 * jp], sn = fs.rt[2 * jp + 1];
