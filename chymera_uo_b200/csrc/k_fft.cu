@@ -8,13 +8,16 @@
 // moments, boundary synthesis).
 //
 // One CTA owns TC adjacent (J,K) columns and holds their LMAX samples in
-// shared memory as rows of stride RS = TC+2 doubles: row 2q is Re(z_q) and
-// row 2q+1 is Im(z_q) of the LMAX/2-point complex sequence
-// z_q = rho(2q) + i rho(2q+1) that POT3 builds (pot/pot3.f:95-98).  Global
-// loads and stores run along J, the fastest dimension of the reference's
-// arrays, so they are coalesced.  The stage structure is fixed at compile time
-// per LMAX; the rotations, output permutation and REALTR recurrence values are
-// the recorded tables, staged in shared memory.
+// shared memory.  The forward tile has rows of stride RS = TC+2 doubles: row
+// 2q is Re(z_q) and row 2q+1 is Im(z_q) of the LMAX/2-point complex sequence
+// z_q = rho(2q) + i rho(2q+1) that POT3 builds (pot/pot3.f:95-98).  The
+// inverse tile has rows of stride TC in split layout: Re(z_q) in row q, Im(z_q)
+// in row IM0+q.  Tiles arrive as TMA boxes of tensor maps over RHO and X
+// (16-byte aligned rows), else as asynchronous copies; global stores run along
+// J, the fastest dimension of the reference's arrays, so they are coalesced.
+// The stage structure is fixed at compile time per LMAX; the rotations, output
+// permutation and REALTR recurrence values are the recorded tables, staged in
+// shared memory.
 #include "devplan.h"
 
 #include <cuda.h>
