@@ -97,7 +97,10 @@ void chy_plan_destroy(chy_plan *p);
  * rho/phi are device pointers (CHY_PTR_DEVICE) or host pointers
  * (CHY_PTR_HOST; pinned memory gives full copy bandwidth).  stream may be
  * NULL (legacy default stream).  diag may be NULL.  For device pointers the
- * call is asynchronous unless diag is non-NULL. */
+ * call is asynchronous unless diag is non-NULL.  Device RHO arrays that start
+ * on a 16-byte boundary (cudaMalloc and torch allocations do) with JMAX even
+ * are read through tensor-memory-access copies; others through 8-byte copies,
+ * with bitwise the same results. */
 int chy_solve(chy_plan *p, const double *rho, double *phi, chy_diag *diag, int ptr_kind,
               void *stream);
 
