@@ -19,6 +19,9 @@
 
 #include <cstdint>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cuda_runtime.h>
 
 namespace chy {
@@ -108,6 +111,10 @@ struct SourceDev {
 // first time a launch needs it; the attribute persists, so later launches make
 // no runtime call (a per-launch cudaFuncSetAttribute stalls the issue stream).
 cudaError_t ensure_smem(const void *kernel, size_t bytes);
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on the driver library); null when unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 // kernels (k_fft.cu, k_bdy.cu, k_solve.cu)
 cudaError_t launch_forward(const DevTables &t, const BatchPtrs &bp, const Work &w, int nb, cudaStream_t s);

@@ -20,9 +20,6 @@
 // shared memory.
 #include "devplan.h"
 
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include <cstring>
 #include <type_traits>
 
@@ -919,8 +916,7 @@ __global__ void k_diag(DevTables t, Work w)
 template <int L>
 static size_t tile_bytes() { return (size_t)Tile<L>::ROWS * Tile<L>::RS * sizeof(double); }
 
-// cuTensorMapEncodeTiled from the driver, through the runtime
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
     static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void *f = nullptr;
@@ -946,7 +942,7 @@ static cudaError_t forward_l(const DevTables &t, const BatchPtrs &bp, const Work
     for (int i = 0; i < nb; ++i) vec16 = vec16 && reinterpret_cast<uintptr_t>(bp.rho[i]) % 16 == 0;
     // with 16-byte aligned rows, the tiles come through one tensor map per
     // solve (encoded here: host arithmetic only, passed by value)
-    RhoMaps maps;
+    RhoMaps maps{};
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (vec16 && enc) {
         bool ok = true;

@@ -1225,24 +1225,6 @@ size_t chy_mixed_work_doubles(const chy_plan *p)
     return (size_t)hp.L * 16 * p->max_batch + 8;
 }
 
-// cuTensorMapEncodeTiled from the driver, through the runtime (no link-time
-// dependency on the driver library).
-static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void *f = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-        else
-            cudaGetLastError();
-    }
-    return fn;
-}
-
 void chy_mixed_bind_work(chy_plan *p, double *base)
 {
     if (!p->mx) p->mx = new MixedState();
