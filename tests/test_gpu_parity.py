@@ -151,6 +151,33 @@ def test_other_grid_sizes(chylib, J, K, L):
         assert rel_l2(phi[ws], ref[ws]) < tol, prec
 
 
+def test_copy_paths_match_tensor_map_paths(chylib):
+    """The transforms read RHO and X through tensor-map tiles when rows are
+    16-byte aligned and JMAX is even, else through 8-byte copies:
+      * JMAX = 65 runs the copy paths of both transforms, held to the oracle
+        like the other grid sizes;
+      * an RHO array 8 bytes past a 16-byte boundary runs the forward
+        transform's copy path, and PHI equals the aligned array's bit for bit."""
+    import torch
+    J, K, L = 65, 32, 64
+    rho, ref, _, _ = oracle_result((J, K, L), seed_override=23)
+    phi, _, _ = gpu_solve(chylib, rho, J, K, L, "fp64")
+    ws = write_set(J, K)
+    assert rel_l2(phi[ws], ref[ws]) < 2e-12
+    J, K, L = 64, 32, 64
+    rho = synth.disk_density(J, K, L, 3, spiral=True, spectrum=True)
+    for prec in ("fp64", "mixed"):
+        plan = chylib.Plan(chylib.grid(J, K, L), prec, 1)
+        a = chylib.to_cuda_fortran(rho)
+        flat = torch.zeros(rho.size + 1, dtype=torch.float64, device="cuda")
+        u = flat[1:].view(L, K + 2, J + 2).permute(2, 1, 0)
+        u.copy_(a)
+        assert u.data_ptr() % 16 == 8
+        pa, pu = plan.solve(a), plan.solve(u)
+        torch.cuda.synchronize()
+        assert torch.equal(pa, pu), prec
+
+
 def test_batch_results_equal_single_solves_bitwise(chylib):
     """Each result is the same alone and in a batch: every reduction has a
     fixed order, nothing depends on scheduling."""
