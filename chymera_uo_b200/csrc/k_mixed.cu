@@ -16,7 +16,8 @@
 //
 // One CTA owns one mode at a time (persistent over (solve, mode) items) and
 // keeps the mode's operand tiles in shared memory and its accumulators in
-// tensor memory; only Y, x and the eigenbasis tiles move through L2.
+// tensor memory; only Y, x, the eigenbasis tiles and the mode's slices of the
+// radial sweep table move through L2.
 // No TMA multicast is used anywhere.  Every wait is bounded: on a timeout the
 // kernel records an error word, stops issuing work, releases its tensor
 // memory and returns.
