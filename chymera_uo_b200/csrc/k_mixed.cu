@@ -1129,7 +1129,7 @@ bool chy_mixed_supported(const chy::HostPlan *hp)
 // Rows [0, h) are eliminated top-down, rows [h, M) bottom-up,
 // h = 32 ceil(M / 64).  They do not depend on the data, so they are formed
 // once, in FP64, here.
-static std::vector<float> sweep_table(const chy::HostPlan &hp)
+std::vector<float> chy::mixed_sweep_table(const chy::HostPlan &hp)
 {
     const int M = hp.M, NT = round64(hp.J), n = hp.N, h = 32 * ((M + 63) / 64);
     const size_t plane = (size_t)(n + 1) * NT * 128;
@@ -1198,7 +1198,7 @@ size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image)
     std::memcpy(image->data() + off2, lam.data(), lam.size() * sizeof(float));
     // radial sweep coefficients, then the sweep table at the next 256-byte
     // boundary
-    const std::vector<float> sw = sweep_table(*hp);
+    const std::vector<float> sw = chy::mixed_sweep_table(*hp);
     size_t off3 = (image->size() + 255) & ~(size_t)255;
     image->resize(off3 + sw.size() * sizeof(float));
     std::memcpy(image->data() + off3, sw.data(), sw.size() * sizeof(float));

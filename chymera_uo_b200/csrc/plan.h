@@ -111,4 +111,8 @@ int build_host_plan(const chy_grid &g, HostPlan &hp, std::string &err);
 // column-major eigenvectors.  Returns 0 or the index that failed to converge.
 int tridiag_eigen(int n, double *d, double *e, double *z);
 
+// The mixed path's radial sweep table of a grid (k_mixed.cu): two FP32
+// planes [N+1][64 ceil(JMAX/64)][128], multipliers then pivot reciprocals.
+std::vector<float> mixed_sweep_table(const HostPlan &hp);
+
 }  // namespace chy

@@ -71,6 +71,54 @@ def test_stencil_matches_pot3_formulas(chylib):
     assert sc[2] == op["cmmax"] and sc[3] == op["ammin"] and sc[4] == op["cnmax"]
 
 
+@pytest.mark.parametrize("J,K,L", [(64, 32, 64), (80, 32, 64), (256, 128, 32)])
+def test_mixed_sweep_table_is_the_two_sided_elimination(chylib, J, K, L):
+    """The mixed path's radial sweep table, restated with the same FP64
+    operations.  For each m and vertical eigenvalue lam_p (-1 on padding
+    rows): the excess g_j = 2 (XLAMM(m) - 1) CC_j, plus the axis term in row
+    1 and -CMMAX in row M; rows j < h eliminated top-down
+    (t = g_j + lam - AM_j e, 1/D = 1/(t - CM_j), e = t/D), rows j >= h
+    bottom-up with AM and CM exchanged, h = 32 ceil(M/64).  The table holds
+    the multipliers, then the pivot reciprocals, as FP32 planes [m][j][p]
+    with JMAX rounded up to 64 rows; rows past M are zero."""
+    g = chylib.grid(J, K, L)
+    M, NZ, N, NT = J - 1, K - 1, L // 2, 64 * ((J + 63) // 64)
+    h = 32 * ((M + 63) // 64)
+    plane = (N + 1) * NT * 128
+    tab = table(chylib, g, "sweep", 2 * plane)
+    assert tab.size == 2 * plane
+    mul = tab[:plane].reshape(N + 1, NT, 128)
+    piv = tab[plane:].reshape(N + 1, NT, 128)
+    am, cm, cc = (table(chylib, g, n, 4096) for n in ("am", "cm", "cc"))
+    xlamm = table(chylib, g, "xlamm", 4096)
+    lam = np.full(128, -1.0)
+    lam[:NZ] = table(chylib, g, "lam", 4096)
+    sc = table(chylib, g, "scalars", 8)
+    cmmax, ammin = sc[2], sc[3]
+    want_mul = np.zeros((N + 1, NT, 128))
+    want_piv = np.zeros((N + 1, NT, 128))
+    for m in range(N + 1):
+        xl2 = 2.0 * (xlamm[m] - 1.0)
+        axis = ((-1.0 if m & 1 else 1.0) - 1.0) * ammin
+        gv = xl2 * cc
+        gv[0] = axis + gv[0]
+        gv[M - 1] = gv[M - 1] - cmmax
+        e = np.zeros(128)
+        for j in range(h):
+            t = (gv[j] + lam) - am[j] * e
+            r = 1.0 / (t - cm[j])
+            e = t * r
+            want_mul[m, j], want_piv[m, j] = e, r
+        f = np.zeros(128)
+        for j in range(M - 1, h - 1, -1):
+            t = (gv[j] + lam) - cm[j] * f
+            r = 1.0 / (t - am[j])
+            f = t * r
+            want_mul[m, j], want_piv[m, j] = f, r
+    assert np.array_equal(mul, want_mul.astype(np.float32).astype(np.float64))
+    assert np.array_equal(piv, want_piv.astype(np.float32).astype(np.float64))
+
+
 def test_boundary_splits_are_sorted_ring_counts(chylib):
     """jk_split = number of rings with RSPHER <= RBDY(JK) (pot/boundary.f:561),
     counted on the reference's own FP64 expressions."""
