@@ -62,6 +62,7 @@ extern "C" long long chy_dbg_table(const chy_grid *g, const char *name, double *
     if (n == "sub_start") return put(hp.sub_start, out, cap);
     if (n == "jk_sub") return put(hp.jk_sub, out, cap);
     if (n == "sweep") return put(mixed_sweep_table(hp), out, cap);
+    if (n == "umma_tiles") return put(mixed_operand_tiles(hp), out, cap);
     if (n == "scalars") {
         std::vector<double> v = {hp.sf1, hp.pig4, hp.cmmax, hp.ammin, hp.cnmax, (double)hp.nkeep,
                                  (double)hp.ncol, (double)(hp.sub_start.size() - 1)};

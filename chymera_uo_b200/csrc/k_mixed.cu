@@ -1205,6 +1205,23 @@ size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image)
     return off;   // lam and the sweep table follow at 256-byte boundaries
 }
 
+std::vector<double> chy::mixed_operand_tiles(const chy::HostPlan &hp)
+{
+    std::vector<char> image;
+    const size_t off = chy_mixed_pack_tables(&hp, &image);
+    std::vector<double> out((size_t)4 * kTiles * kTiles);
+    for (int t = 0; t < 4; ++t) {
+        const size_t base = off + (size_t)(t >> 1) * kAImg + (size_t)(t & 1) * kTiles * kTiles * 2;
+        for (int r = 0; r < kTiles; ++r)
+            for (int k = 0; k < kTiles; ++k) {
+                __half h;
+                std::memcpy(&h, image.data() + base + kmaj_off(r, k, kTiles), 2);
+                out[((size_t)t * kTiles + r) * kTiles + k] = (double)__half2float(h);
+            }
+    }
+    return out;
+}
+
 void chy_mixed_bind_tables(chy_plan *p, char *dev_base)
 {
     if (!p->mx) p->mx = new MixedState();

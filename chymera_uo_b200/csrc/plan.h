@@ -114,5 +114,8 @@ int tridiag_eigen(int n, double *d, double *e, double *z);
 // The mixed path's radial sweep table of a grid (k_mixed.cu): two FP32
 // planes [N+1][64 ceil(JMAX/64)][128], multipliers then pivot reciprocals.
 std::vector<float> mixed_sweep_table(const HostPlan &hp);
+// Its eigenbasis operand tiles read back through their swizzled layout:
+// [U hi, U lo, V hi, V lo], each [128 rows][128 K] (test hook).
+std::vector<double> mixed_operand_tiles(const HostPlan &hp);
 
 }  // namespace chy

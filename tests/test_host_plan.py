@@ -119,6 +119,29 @@ def test_mixed_sweep_table_is_the_two_sided_elimination(chylib, J, K, L):
     assert np.array_equal(piv, want_piv.astype(np.float32).astype(np.float64))
 
 
+@pytest.mark.parametrize("J,K,L", [(64, 32, 64), (128, 128, 64)])
+def test_mixed_operand_tiles_are_hi_lo_splits(chylib, J, K, L):
+    """The eigenbasis operands of the tensor-core products, read back through
+    their K-major 128-byte-swizzled layout: hi = fp16(2^12 U(p,k)) and
+    lo = fp16(2^12 U(p,k) - hi) with rows p and K index k, the same for
+    V(k,p) with rows k and K index p, zero outside NZ x NZ; hi + lo carries
+    2^12 U to about 22 bits."""
+    g = chylib.grid(J, K, L)
+    NZ = K - 1
+    tiles = table(chylib, g, "umma_tiles", 4 * 128 * 128).reshape(4, 128, 128)
+    U = table(chylib, g, "U", NZ * NZ).reshape(NZ, NZ)   # U[p][k]
+    V = table(chylib, g, "V", NZ * NZ).reshape(NZ, NZ)   # V[k][p]
+    for t, A in ((0, U), (2, V)):
+        v = 4096.0 * A
+        hi = v.astype(np.float16).astype(np.float64)
+        lo = (v - hi).astype(np.float16).astype(np.float64)
+        assert np.array_equal(tiles[t, :NZ, :NZ], hi)
+        assert np.array_equal(tiles[t + 1, :NZ, :NZ], lo)
+        for q in (t, t + 1):
+            assert not tiles[q, NZ:, :].any() and not tiles[q, :, NZ:].any()
+        assert np.max(np.abs(hi + lo - v)) <= 2.0 ** -21 * np.max(np.abs(v))
+
+
 def test_boundary_splits_are_sorted_ring_counts(chylib):
     """jk_split = number of rings with RSPHER <= RBDY(JK) (pot/boundary.f:561),
     counted on the reference's own FP64 expressions."""
