@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(_HERE, "libchy_pot3.so")
 CHY_OK = 0
 CHY_PREC_FP64 = 0
 CHY_PREC_MIXED = 1
+CHY_PREC_FP64_BLKTRI = 2
 CHY_PTR_DEVICE = 0
 CHY_PTR_HOST = 1
 CHY_LITERAL_GCC = 0
@@ -127,6 +128,8 @@ def lib():
         L.chy_dbg_realtr.restype = i
         L.chy_dbg_table.argtypes = [C.POINTER(ChyGrid), C.c_char_p, C.POINTER(C.c_double), ll]
         L.chy_dbg_table.restype = ll
+        L.chy_dbg_blktri.argtypes = [C.POINTER(ChyGrid), i, C.POINTER(C.c_double)]
+        L.chy_dbg_blktri.restype = i
         L.chy_dbg_work.argtypes = [vp, C.c_char_p, C.POINTER(C.c_double), ll]
         L.chy_dbg_work.restype = ll
         L.chy_dbg_umma.argtypes = [vp, i, vp, vp, i]
@@ -183,6 +186,18 @@ def _is_cuda_tensor(x) -> bool:
     return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
 
 
+PRECISIONS = {"fp64": CHY_PREC_FP64, "mixed": CHY_PREC_MIXED, "blktri": CHY_PREC_FP64_BLKTRI}
+
+
+def precision_code(precision: str) -> int:
+    """CHY_PREC_* of a precision name: "blktri" (the reference's BLKTRI
+    cyclic reduction in FP64, its rounding), "fp64" (FP64 eigenbasis solve)
+    or "mixed" (tensor cores + FP64 refinement)."""
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, not {precision!r}")
+    return PRECISIONS[precision]
+
+
 class Plan:
     """Per-grid tables + device work space for up to ``max_batch`` solves."""
 
@@ -191,7 +206,7 @@ class Plan:
         self.precision = precision
         self.shape = (g.jmax + 2, g.kmax + 2, g.lmax)
         p = C.c_void_p()
-        prec = CHY_PREC_MIXED if precision == "mixed" else CHY_PREC_FP64
+        prec = precision_code(precision)
         _check(lib().chy_plan_create(C.byref(g), prec, max_batch, C.byref(p)))
         self._p = p
         self.max_batch = max_batch
@@ -347,8 +362,7 @@ class Server:
 
     def __init__(self, precision: str = "mixed", hbm_budget: int = 0, max_batch: int = 8,
                  arena_fraction: float = 0.5):
-        o = ServerOpts(hbm_budget, CHY_PREC_MIXED if precision == "mixed" else CHY_PREC_FP64, max_batch,
-                       arena_fraction)
+        o = ServerOpts(hbm_budget, precision_code(precision), max_batch, arena_fraction)
         p = C.c_void_p()
         _check(lib().chy_server_create(C.byref(o), C.byref(p)))
         self._p = p

@@ -28,7 +28,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                       "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
                       "-I" + INC, "-I" + CSRC]
-NOFMA = {"k_fft.cu", "k_bdy.cu", "k_source.cu"}
+NOFMA = {"k_fft.cu", "k_bdy.cu", "k_source.cu", "k_blktri.cu"}
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
              "-I" + INC, "-I" + CSRC]
 

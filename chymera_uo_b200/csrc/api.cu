@@ -127,7 +127,8 @@ void chy_plan_destroy(chy_plan *p)
 int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **out)
 {
     if (!g || !out || max_batch < 1) return fail(CHY_ERR_ARG, "null descriptor/output or max_batch < 1");
-    if (precision != CHY_PREC_FP64 && precision != CHY_PREC_MIXED) return fail(CHY_ERR_ARG, "unknown precision");
+    if (precision != CHY_PREC_FP64 && precision != CHY_PREC_MIXED && precision != CHY_PREC_FP64_BLKTRI)
+        return fail(CHY_ERR_ARG, "unknown precision");
     *out = nullptr;
     chy_plan *p = new (std::nothrow) chy_plan();
     if (!p) return fail(CHY_ERR_NOMEM, "host allocation");
@@ -144,6 +145,16 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     p->precision = precision;
     p->max_batch = max_batch;
     const HostPlan &hp = p->hp;
+    BlkSchedule bs;
+    if (precision == CHY_PREC_FP64_BLKTRI) {
+        // BLKTRI(IFLG=0) (pot/blktri.f:13-46): COMPB's roots and the recorded
+        // cyclic-reduction schedule
+        st = build_blk_schedule(hp.an, hp.bn, hp.cn, hp.M, bs, err);
+        if (st != 0) {
+            delete p;
+            return fail(st == 1 ? CHY_ERR_M_LT_2 : st == 2 ? CHY_ERR_N_NOT_POW2 : CHY_ERR_EIGEN, err);
+        }
+    }
 
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
@@ -167,6 +178,14 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     size_t o_am = pk.vec(hp.am), o_cmv = pk.vec(hp.cm), o_cc = pk.vec(hp.cc), o_bm0 = pk.vec(hp.bm0), o_xl = pk.vec(hp.xlamm);
     size_t o_an = pk.vec(hp.an), o_bn = pk.vec(hp.bn), o_cn = pk.vec(hp.cn);
     size_t o_U = pk.vec(hp.U), o_V = pk.vec(hp.V), o_lam = pk.vec(hp.lam);
+    size_t o_bst = 0, o_bpg = 0, o_btk = 0, o_bsg = 0, o_bmt = 0;
+    if (precision == CHY_PREC_FP64_BLKTRI) {
+        o_bst = pk.vec(bs.steps);
+        o_bpg = pk.vec(bs.progs);
+        o_btk = pk.vec(bs.tasks);
+        o_bsg = pk.vec(bs.stages);
+        o_bmt = pk.vec(blk_bm_table(hp));
+    }
     size_t o_ext = chy_mixed_pack_tables(&hp, &pk.host);
     p->table_bytes = pk.host.size();
     ce = cudaMalloc(&p->d_tables, p->table_bytes);
@@ -211,6 +230,16 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     t.an = (const double *)(D + o_an); t.bn = (const double *)(D + o_bn); t.cn = (const double *)(D + o_cn);
     t.U = (const double *)(D + o_U); t.V = (const double *)(D + o_V); t.lam = (const double *)(D + o_lam);
     for (int i = 0; i < 11; i++) t.zx[i] = hp.zx[i];
+    if (precision == CHY_PREC_FP64_BLKTRI) {
+        t.blk.nvec = bs.nvec;
+        t.blk.nstage = (int)bs.stages.size();
+        t.blk.nblk = hp.L >= 32 ? hp.L / 32 : 1;
+        t.blk.steps = (const BlkStep *)(D + o_bst);
+        t.blk.progs = (const BlkProg *)(D + o_bpg);
+        t.blk.tasks = (const BlkTask *)(D + o_btk);
+        t.blk.stages = (const BlkStage *)(D + o_bsg);
+        t.blk.bmt = (const double *)(D + o_bmt);
+    }
     chy_mixed_bind_tables(p, D + o_ext);
 
     // ---- work space
@@ -227,9 +256,12 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     w.sdiag = (size_t)kDiagPart + 2 * (size_t)hp.L;
     // every array starts on a 256-byte boundary (16-byte async copies read them)
     auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };
+    const bool blk = precision == CHY_PREC_FP64_BLKTRI;
+    const size_t nbvec = blk ? al(blk_vector_doubles(t, max_batch)) : 0;
+    const size_t nbscr = blk ? al(blk_scratch_doubles(t, max_batch, p->num_sms)) : 0;
     const size_t per = al(w.sX * max_batch) + al(w.sW * max_batch) + al(w.sC * max_batch) +
                        al(w.smom * max_batch) + al(w.ssub * max_batch) + al(w.sscan * max_batch) +
-                       al(w.sphac * max_batch) + al(w.sdiag * max_batch);
+                       al(w.sphac * max_batch) + al(w.sdiag * max_batch) + nbvec + nbscr;
     size_t ext = chy_mixed_work_doubles(p);
     p->work_bytes = (per + ext) * sizeof(double) + 4096;
     ce = cudaMalloc(&p->d_work, p->work_bytes);
@@ -246,6 +278,8 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     w.scan = q; q += al(w.sscan * max_batch);
     w.phac = q; q += al(w.sphac * max_batch);
     w.diag = q; q += al(w.sdiag * max_batch);
+    w.bvec = blk ? q : nullptr; q += nbvec;
+    w.bscr = blk ? q : nullptr; q += nbscr;
     w.coef = nullptr;
     chy_mixed_bind_work(p, q);
     CHY_CUDA(cudaMemset(p->d_work, 0, p->work_bytes));
@@ -392,6 +426,7 @@ long long chy_plan_bytes_per_solve(const chy_plan *p)
     if (!p) return 0;
     const Work &w = p->w;
     size_t per = w.sX + w.sW + w.sC + w.smom + w.ssub + w.sscan + w.sphac + w.sdiag;
+    if (p->precision == CHY_PREC_FP64_BLKTRI) per += (size_t)p->t.blk.nvec * p->t.M * p->t.L;
     return (long long)(per * sizeof(double));
 }
 
@@ -469,6 +504,8 @@ static int run_batch(chy_plan *p, const BatchPtrs &bp, int nb, cudaStream_t s)
     if (p->precision == CHY_PREC_FP64) {
         CHY_CUDA(launch_solve_fp64(t, p->w, nb, p->num_sms, s));
         nl = 3;
+    } else if (p->precision == CHY_PREC_FP64_BLKTRI) {
+        CHY_CUDA(launch_solve_blk(t, p->w, nb, p->num_sms, s, &nl));
     } else {
         int st = chy_mixed_solve(p, nb, s, &nl);
         if (st != CHY_OK) return st;

@@ -3,6 +3,7 @@
 #include <string>
 #include <vector>
 
+#include "blk.h"
 #include "chy_pot3_testing.h"
 #include "plan.h"
 
@@ -62,6 +63,17 @@ extern "C" long long chy_dbg_table(const chy_grid *g, const char *name, double *
     if (n == "sub_start") return put(hp.sub_start, out, cap);
     if (n == "jk_sub") return put(hp.jk_sub, out, cap);
     if (n == "sweep") return put(mixed_sweep_table(hp), out, cap);
+    if (n == "blk_roots" || n == "blk_cns") {
+        BlkSchedule bs;
+        if (build_blk_schedule(hp.an, hp.bn, hp.cn, hp.M, bs, err) != 0) return -CHY_ERR_EIGEN;
+        return put(n == "blk_roots" ? bs.roots : bs.cns, out, cap);
+    }
+    if (n == "blk_bm") {
+        std::vector<double> v((size_t)hp.L * hp.M);
+        for (int l = 0; l < hp.L; l++) blk_mode_bm(hp, l, v.data() + (size_t)l * hp.M);
+        return put(v, out, cap);
+    }
+    if (n == "blk_bm_table") return put(blk_bm_table(hp), out, cap);
     if (n == "umma_tiles") return put(mixed_operand_tiles(hp), out, cap);
     if (n == "scalars") {
         std::vector<double> v = {hp.sf1, hp.pig4, hp.cmmax, hp.ammin, hp.cnmax, (double)hp.nkeep,
@@ -69,4 +81,21 @@ extern "C" long long chy_dbg_table(const chy_grid *g, const char *name, double *
         return put(v, out, cap);
     }
     return -CHY_ERR_ARG;
+}
+
+extern "C" int chy_dbg_blktri(const chy_grid *g, int l, double *y)
+{
+    if (!g || !y) return CHY_ERR_ARG;
+    HostPlan hp;
+    std::string err;
+    int st = build_host_plan(*g, hp, err);
+    if (st != CHY_OK) return st;
+    if (l < 0 || l >= hp.L) return CHY_ERR_ARG;
+    BlkSchedule bs;
+    st = build_blk_schedule(hp.an, hp.bn, hp.cn, hp.M, bs, err);
+    if (st != 0) return st == 1 ? CHY_ERR_M_LT_2 : st == 2 ? CHY_ERR_N_NOT_POW2 : CHY_ERR_EIGEN;
+    std::vector<double> bm(hp.M);
+    blk_mode_bm(hp, l, bm.data());
+    blk_solve_host(bs, hp.am.data(), bm.data(), hp.cm.data(), y);
+    return CHY_OK;
 }

@@ -15,6 +15,10 @@
 //   PHAC [K+2]             ZAXPHI deviations
 //   DIAG [8 + 2L]          TMASS, PHICHK, KLOCAT, -, INDIRECTX, INDIRECTY, -, -,
 //                          then per-L partial mass moments of the INDIRECT shift.
+// BLKTRI-order FP64 path only (k_blktri.cu), not per solve but per group of
+// 32 (solve, mode) items, item = solve * L + mode:
+//   BVEC [group][NVEC][M][32] FP64 each item's BLKTRI vectors, lane-interleaved
+//   BSCR [cta][warp][2][M][32] FP64 PRDCT's elimination scratch (W, D)
 #pragma once
 
 #include <cstdint>
@@ -23,6 +27,8 @@
 #include <cudaTypedefs.h>
 
 #include <cuda_runtime.h>
+
+#include "blk.h"
 
 namespace chy {
 
@@ -42,6 +48,17 @@ struct FftDev {
 // True when the device kernels' compile-time stage structure for this LMAX
 // equals the recorded schedule.
 bool fft_shape_supported(const FftDev &f, int L);
+
+// The recorded BLKTRI schedule (blk.h) and BM of every mode, laid out
+// [mode block][j][32 lanes] with lane -> mode (32 * block + lane) mod L.
+struct BlkDev {
+    int nvec, nstage, nblk;
+    const BlkStep *steps;
+    const BlkProg *progs;
+    const BlkTask *tasks;
+    const BlkStage *stages;
+    const double *bmt;
+};
 
 struct DevTables {
     int J, K, L, N, M, NZ, nring, nkeep, njk, ncol, nsub, ntrm, maxtrm, isyma, npoint;
@@ -65,6 +82,7 @@ struct DevTables {
     // vertical eigenbasis, row-major [NZ][NZ]: U(p,k) and V(k,p)
     const double *U, *V, *lam;
     double zx[11];
+    BlkDev blk;                     // CHY_PREC_FP64_BLKTRI plans only
 };
 
 // Per-launch batch addressing.  Caller arrays come as pointer lists; the
@@ -78,6 +96,7 @@ struct Work {
     double *X, *W, *C, *mom, *sub, *scan, *phac, *diag;
     size_t sX, sW, sC, smom, ssub, sscan, sphac, sdiag;   // per-solve strides (elements)
     double *coef;                                    // optional /COEFS/ output (solve 0 only)
+    double *bvec, *bscr;                             // BLKTRI-order path (k_blktri.cu)
 };
 
 // ExternalPot (pot/ExternalPot.f:1-80): the star potential added after POT3.
@@ -121,6 +140,11 @@ cudaError_t launch_forward(const DevTables &t, const BatchPtrs &bp, const Work &
 cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStream_t s);
 cudaError_t launch_bdy_synth(const DevTables &t, const Work &w, int nb, cudaStream_t s);
 cudaError_t launch_solve_fp64(const DevTables &t, const Work &w, int nb, int num_sms, cudaStream_t s);
+// BLKTRI-order FP64 mode solves (k_blktri.cu): gather, cyclic reduction, scatter.
+cudaError_t launch_solve_blk(const DevTables &t, const Work &w, int nb, int num_sms, cudaStream_t s, int *launches);
+// Its work-space sizes in doubles: BVEC for nb solves, BSCR for a plan of max_batch.
+size_t blk_vector_doubles(const DevTables &t, int nb);
+size_t blk_scratch_doubles(const DevTables &t, int max_batch, int num_sms);
 // Inverse transform into PHI (plus STARPHI when x.on) and the diagnostics;
 // with x.on also the cells POT3 leaves alone; reports its launch count.
 cudaError_t launch_inverse(const DevTables &t, const BatchPtrs &bp, const Work &w, const StarDev &x, int nb,

@@ -1,0 +1,243 @@
+// k_blktri.cu -- POT3's mode solves in the reference's own algorithm and
+// order: FISHPACK BLKTRI generalized cyclic reduction (pot/blktri.f:60-260),
+// FP64, replayed from the schedule recorded on the host (blk.h).
+//
+// Work items are (solve, mode) pairs, 32 to a group: one lane of a warp per
+// item.  Every item of a group runs the same stage/task/program sequence
+// (the schedule does not depend on the mode), so a warp's lanes never
+// diverge; only BM, the radial diagonal, differs between lanes.  Each item's
+// vectors (Y(:,1..N) and the intermediate products, M doubles each) are
+// stored lane-interleaved, [group][vector][j][lane], so every access of a
+// warp is one contiguous 256-byte run.
+//
+// One CTA owns a group at a time and walks the stages; the tasks of a stage
+// are independent PRDCT calls (or element-wise combinations) spread over the
+// CTA's warps, with a barrier between stages.  A PRDCT call keeps its
+// elimination multipliers D and partial solution W in per-warp scratch.
+//
+// This file is compiled with --fmad=false and uses IEEE division: every
+// product, sum and quotient rounds as the reference's, so the modes equal
+// the reference's BLKTRI output bit for bit.
+#include "devplan.h"
+
+namespace chy {
+
+constexpr int kBlkLanes = 32;
+constexpr int kBlkUnroll = 8;   // rows whose loads are issued ahead of the recurrence
+
+// Y(j,k) = 4 pi G Xhat(j,k) - boundary folds (pot/pot3.f:212-224), in that
+// order of operations.
+__device__ __forceinline__ double blk_rhs(const DevTables &t, const double *Xl, int j, int k)
+{
+    double y = t.pig4 * Xl[(size_t)k * t.J + j];
+    if (k == t.NZ - 1) y = y - t.cnmax * Xl[(size_t)t.NZ * t.J + j];
+    if (j == t.M - 1) y = y - t.cmmax * Xl[(size_t)k * t.J + t.M];
+    return y;
+}
+
+// X (mode-major) -> lane-interleaved right-hand sides Y(:,k+1) of every item
+// of group g.  Grid (groups, NZ); a 32 x 32 tile per pass.
+__global__ void __launch_bounds__(256) k_blk_gather(DevTables t, Work w, int nb)
+{
+    __shared__ double tile[kBlkLanes][kBlkLanes + 1];
+    const int g = blockIdx.x, k = blockIdx.y, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int M = t.M, L = t.L;
+    const BlkDev &d = t.blk;
+    double *out = w.bvec + ((size_t)g * d.nvec + k) * (size_t)M * kBlkLanes;
+    for (int j0 = 0; j0 < M; j0 += kBlkLanes) {
+        for (int r = ty; r < kBlkLanes; r += 8) {
+            const int item = g * kBlkLanes + r, b = item / L, l = item % L, j = j0 + tx;
+            double v = 0.0;
+            if (b < nb && j < M) v = blk_rhs(t, w.X + (size_t)b * w.sX + (size_t)l * t.K * t.J, j, k);
+            tile[r][tx] = v;
+        }
+        __syncthreads();
+        for (int jj = ty; jj < kBlkLanes; jj += 8) {
+            const int j = j0 + jj;
+            if (j < M) out[(size_t)j * kBlkLanes + tx] = tile[tx][jj];
+        }
+        __syncthreads();
+    }
+}
+
+// Solved Y(:,k+1) of every item of group g -> interior of X.
+__global__ void __launch_bounds__(256) k_blk_scatter(DevTables t, Work w, int nb)
+{
+    __shared__ double tile[kBlkLanes][kBlkLanes + 1];
+    const int g = blockIdx.x, k = blockIdx.y, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int M = t.M, L = t.L;
+    const BlkDev &d = t.blk;
+    const double *in = w.bvec + ((size_t)g * d.nvec + k) * (size_t)M * kBlkLanes;
+    for (int j0 = 0; j0 < M; j0 += kBlkLanes) {
+        for (int jj = ty; jj < kBlkLanes; jj += 8) {
+            const int j = j0 + jj;
+            tile[tx][jj] = (j < M) ? in[(size_t)j * kBlkLanes + tx] : 0.0;
+        }
+        __syncthreads();
+        for (int r = ty; r < kBlkLanes; r += 8) {
+            const int item = g * kBlkLanes + r, b = item / L, l = item % L, j = j0 + tx;
+            if (b < nb && j < M) w.X[(size_t)b * w.sX + (size_t)l * t.K * t.J + (size_t)k * t.J + j] = tile[r][tx];
+        }
+        __syncthreads();
+    }
+}
+
+// One PRDCT call (pot/blktri.f:177-260) for the 32 items of a warp.  Vector
+// pointers are already offset to the lane; consecutive rows are 32 apart.
+__device__ __forceinline__ void blk_prdct(const BlkProg &pg, const BlkStep *__restrict__ steps,
+                                          const double *__restrict__ X, double *__restrict__ Y,
+                                          double *__restrict__ Wv, double *__restrict__ Dv,
+                                          const double *__restrict__ bm, const double *am, const double *cm, int m)
+{
+    constexpr int S = kBlkLanes, U = kBlkUnroll;
+    // entry: W = X or -X, Y = W, and Y = AA(NA) W when NA > 0 (:183-208)
+    for (int j = 0; j < m; j++) {
+        double v = X[(size_t)j * S];
+        if (pg.neg) v = -v;
+        Y[(size_t)j * S] = pg.pre ? pg.pre_coef * v : v;
+    }
+    for (int q = 0; q < pg.nsteps; q++) {
+        const BlkStep sp = steps[pg.first + q];
+        const double rt = sp.rt;
+        // elimination from row M (:214-221)
+        const double bl = bm[(size_t)(m - 1) * S] - rt;
+        double dn = am[m - 1] / bl;
+        double wn = Y[(size_t)(m - 1) * S] / bl;
+        Dv[(size_t)(m - 1) * S] = dn;
+        Wv[(size_t)(m - 1) * S] = wn;
+        for (int i0 = m - 2; i0 >= 1; i0 -= U) {
+            double yv[U], bv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int i = i0 - u;
+                yv[u] = (i >= 1) ? Y[(size_t)i * S] : 0.0;
+                bv[u] = (i >= 1) ? bm[(size_t)i * S] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int i = i0 - u;
+                if (i >= 1) {
+                    const double den = bv[u] - rt - cm[i] * dn;
+                    dn = am[i] / den;
+                    wn = (yv[u] - cm[i] * wn) / den;
+                    Dv[(size_t)i * S] = dn;
+                    Wv[(size_t)i * S] = wn;
+                }
+            }
+        }
+        // row 1 (:222-228)
+        const double den = bm[0] - rt - cm[0] * dn;
+        double w = (den == 0) ? 1. : (Y[0] - cm[0] * wn) / den;
+        // substitution (:229-231) fused with the right-hand-side update that
+        // follows the pass: Y = W (:234-238), Y = Y + c W (:254-257),
+        // Y = c W (:201-208)
+        const int post = sp.post;
+        const double c = sp.coef;
+        auto put = [&](int j, double v) {
+            if (post == BLK_COPY) Y[(size_t)j * S] = v;
+            else if (post == BLK_AXPY) Y[(size_t)j * S] = Y[(size_t)j * S] + c * v;
+            else if (post == BLK_SCALE) Y[(size_t)j * S] = c * v;
+        };
+        put(0, w);
+        for (int j0 = 1; j0 < m; j0 += U) {
+            double wv[U], dv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = j0 + u;
+                wv[u] = (j < m) ? Wv[(size_t)j * S] : 0.0;
+                dv[u] = (j < m) ? Dv[(size_t)j * S] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = j0 + u;
+                if (j < m) {
+                    w = wv[u] - dv[u] * w;
+                    put(j, w);
+                }
+            }
+        }
+    }
+}
+
+// Persistent CTAs over groups; NW warps per CTA.  Dynamic shared memory
+// holds AM and CM (2 M doubles).
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) k_blk_solve(DevTables t, Work w, int ngroups)
+{
+    extern __shared__ double sm[];
+    const BlkDev &d = t.blk;
+    const int m = t.M, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *am = sm, *cm = sm + m;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        am[i] = t.am[i];
+        cm[i] = t.cm[i];
+    }
+    __syncthreads();
+    const size_t vlen = (size_t)m * kBlkLanes;
+    double *Wv = w.bscr + ((size_t)blockIdx.x * NW + warp) * 2 * vlen + lane;
+    double *Dv = Wv + vlen;
+    for (int g = blockIdx.x; g < ngroups; g += gridDim.x) {
+        double *base = w.bvec + (size_t)g * d.nvec * vlen;
+        const double *bm = d.bmt + (size_t)(g % d.nblk) * vlen + lane;
+        for (int s = 0; s < d.nstage; s++) {
+            const BlkStage st = d.stages[s];
+            if (st.kind == BLK_TASK_PRDCT) {
+                for (int i = warp; i < st.ntasks; i += NW) {
+                    const BlkTask tk = d.tasks[st.first + i];
+                    const BlkProg pg = d.progs[tk.prog];
+                    blk_prdct(pg, d.steps, base + (size_t)tk.a * vlen + lane, base + (size_t)tk.out * vlen + lane,
+                              Wv, Dv, bm, am, cm, m);
+                }
+            } else {
+                const long long total = (long long)st.ntasks * (long long)vlen;
+                for (long long e = threadIdx.x; e < total; e += blockDim.x) {
+                    const BlkTask tk = d.tasks[st.first + (int)(e / (long long)vlen)];
+                    const size_t r = (size_t)(e % (long long)vlen);
+                    const double a = base[(size_t)tk.a * vlen + r];
+                    const double b = tk.b < 0 ? 0.0 : base[(size_t)tk.b * vlen + r];
+                    const double c = tk.c < 0 ? 0.0 : base[(size_t)tk.c * vlen + r];
+                    // Y = W1 + W2 - Y (:106-108); W1 = Y - W1 - W2 (:157-159)
+                    base[(size_t)tk.out * vlen + r] = (st.kind == BLK_TASK_SUMSUB) ? (a + b) - c : (a - b) - c;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+constexpr int kBlkWarps = 8;
+
+static int blk_solve_ctas(int ngroups, int num_sms)
+{
+    const int cap = 2 * num_sms;
+    return ngroups < cap ? ngroups : cap;
+}
+
+static int blk_groups(const DevTables &t, int nb) { return (nb * t.L + kBlkLanes - 1) / kBlkLanes; }
+
+size_t blk_scratch_doubles(const DevTables &t, int max_batch, int num_sms)
+{
+    return (size_t)blk_solve_ctas(blk_groups(t, max_batch), num_sms) * kBlkWarps * 2 * (size_t)t.M * kBlkLanes;
+}
+
+size_t blk_vector_doubles(const DevTables &t, int nb)
+{
+    return (size_t)blk_groups(t, nb) * t.blk.nvec * (size_t)t.M * kBlkLanes;
+}
+
+cudaError_t launch_solve_blk(const DevTables &t, const Work &w, int nb, int num_sms, cudaStream_t s, int *launches)
+{
+    const int ngroups = blk_groups(t, nb);
+    const size_t smem = (size_t)2 * t.M * sizeof(double);
+    cudaError_t e = ensure_smem((const void *)k_blk_solve<kBlkWarps>, smem);
+    if (e != cudaSuccess) return e;
+    k_blk_gather<<<dim3(ngroups, t.NZ), 256, 0, s>>>(t, w, nb);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_blk_solve<kBlkWarps><<<blk_solve_ctas(ngroups, num_sms), kBlkWarps * 32, smem, s>>>(t, w, ngroups);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_blk_scatter<<<dim3(ngroups, t.NZ), 256, 0, s>>>(t, w, nb);
+    if (launches) *launches = 3;
+    return cudaGetLastError();
+}
+
+}  // namespace chy

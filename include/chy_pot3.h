@@ -46,7 +46,21 @@ extern "C" {
 
 /* ---- descriptors --------------------------------------------------------- */
 enum { CHY_LITERAL_GCC = 0, CHY_LITERAL_R8 = 1 };
-enum { CHY_PREC_FP64 = 0, CHY_PREC_MIXED = 1 };
+/* Mode-solve precisions.
+ *   CHY_PREC_FP64_BLKTRI  the reference's own mode solver, FISHPACK BLKTRI
+ *                         generalized cyclic reduction (pot/blktri.f:3-423,
+ *                         called from pot/pot3.f:233-239), in FP64 with the
+ *                         reference's operations in the reference's order:
+ *                         the plain FP64 pot3, equal to the reference's
+ *                         rounding.
+ *   CHY_PREC_FP64         FP64 through the eigenbasis of the m-independent
+ *                         vertical operator and radial Thomas sweeps; several
+ *                         times faster, ~10x closer to the exact solution
+ *                         than BLKTRI's rounding (so a few 1e-12 away from the
+ *                         reference's result on 256 x 128 grids).
+ *   CHY_PREC_MIXED        tensor-core FP16 hi/lo transforms, FP32 sweeps and
+ *                         an FP64 refinement (<= 1e-10 of the reference). */
+enum { CHY_PREC_FP64 = 0, CHY_PREC_MIXED = 1, CHY_PREC_FP64_BLKTRI = 2 };
 enum { CHY_PTR_DEVICE = 0, CHY_PTR_HOST = 1 };
 
 /* Grid and call parameters.  Fields mirror COMMON /GRID/ and /BLOK6/

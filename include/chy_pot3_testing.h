@@ -21,8 +21,15 @@ int chy_dbg_realtr(int n, int isn, int literal_kind, double *a, double *b);
  * "U", "V", "lam", "an", "bn", "cn", "am", "cm", "cc", "bm0", "xlamm",
  * "ring_term" ([ring][66]), "ring_dv", "ring_rsph", "jk_split", "jk_bin",
  * "jk_hout", "sub_start", "jk_sub", "scalars" (sf1, pig4, cmmax, ammin,
- * cnmax, nkeep, ncol, nsub). */
+ * cnmax, nkeep, ncol, nsub), and for the BLKTRI-order path "blk_roots"
+ * (COMPB's root table B), "blk_cns" (CN as BLKTR1 receives it), "blk_bm"
+ * ([mode][j] BM) and "blk_bm_table" (BM as the kernel reads it). */
 long long chy_dbg_table(const chy_grid *g, const char *name, double *out, long long cap);
+
+/* The recorded BLKTRI schedule replayed on the host for mode l of grid g:
+ * y is Y(JMAX-1, KMAX-1) column-major, solved in place with the plan's AM,
+ * BM(l) and CM, exactly as the device kernel does it; no device work. */
+int chy_dbg_blktri(const chy_grid *g, int l, double *y);
 
 /* Copies work array `name` of batch slot 0 ("X", "mom", "sub", "scan",
  * "phac", "diag") to host memory after a device synchronisation; returns the

@@ -237,3 +237,17 @@ def blktri_solve(an, bn, cn, am, bm, cm, y):
         if iflg == 0 and ierr.value != 0:
             return yf, ierr.value
     return yf, ierr.value
+
+
+def blktri_roots(an, bn, cn, m):
+    """The work array of BLKTRI(IFLG=0) (NP=MP=1): COMPB's root table B
+    followed by the shifted CN copy (pot/blktri.f:35-46)."""
+    n = an.shape[0]
+    w = np.zeros(lib().ora_blktri_wsize(m + 1, n + 1) + 4 * n + 64)
+    state = C.create_string_buffer(max(256, lib().ora_blktri_state_size()))
+    ierr = C.c_int(0)
+    y = np.zeros((m, n), order="F")
+    am = np.zeros(m)
+    lib().ora_blktri(C.cast(state, C.c_void_p), 0, 1, n, _dp(an), _dp(bn), _dp(cn), 1, m, _dp(am), _dp(am),
+                     _dp(am), m, _dp(y), C.byref(ierr), _dp(w))
+    return w, ierr.value
