@@ -128,6 +128,8 @@ def lib():
         L.chy_dbg_realtr.restype = i
         L.chy_dbg_table.argtypes = [C.POINTER(ChyGrid), C.c_char_p, C.POINTER(C.c_double), ll]
         L.chy_dbg_table.restype = ll
+        L.chy_dbg_mixed_probe.argtypes = [vp, i]
+        L.chy_dbg_mixed_probe.restype = i
         L.chy_dbg_blktri.argtypes = [C.POINTER(ChyGrid), i, C.POINTER(C.c_double)]
         L.chy_dbg_blktri.restype = i
         L.chy_dbg_work.argtypes = [vp, C.c_char_p, C.POINTER(C.c_double), ll]

@@ -649,7 +649,19 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
     }
     for (int i = 0; i < R; i++)
         if (used[i]) CHY_CUDA(cudaStreamWaitEvent(s, p->ev_out[i], 0));
+    // a bounded wait that expired in any of these mode solves (with diag the
+    // chunks have reported it already)
+    int *err = diag ? nullptr : chy_mixed_host_error_word(p);
+    if (err) {
+        *err = 0;
+        st = chy_mixed_read_error(p, err, s);
+        if (st != CHY_OK) return fail(st, "error word readback");
+    }
     CHY_CUDA(cudaStreamSynchronize(s));
+    if (err && *err != 0) {
+        *err = 0;
+        return fail(CHY_ERR_TIMEOUT, "mode solve: a bounded wait expired; the affected modes of PHI are NaN");
+    }
     return CHY_OK;
 }
 
@@ -861,4 +873,11 @@ extern "C" int chy_solve_static(chy_plan *p, const double *rho, double *phi, voi
     int nv = 0;
     CHY_CUDA(launch_inverse(t, bp, w, StarDev{}, 1, s, &nv));   // POT3 alone
     return CHY_OK;
+}
+
+extern "C" int chy_dbg_mixed_probe(chy_plan *p, int polls)
+{
+    if (!p) return fail(CHY_ERR_ARG, "null plan");
+    const int st = chy_dbg_mixed_probe_set(p, polls);
+    return st == CHY_OK ? st : fail(st, "probe needs a mixed plan and polls >= 0");
 }

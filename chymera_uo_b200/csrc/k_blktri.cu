@@ -91,6 +91,7 @@ __device__ __forceinline__ void blk_prdct(const BlkProg &pg, const BlkStep *__re
 {
     constexpr int S = kBlkLanes, U = kBlkUnroll;
     // entry: W = X or -X, Y = W, and Y = AA(NA) W when NA > 0 (:183-208)
+#pragma unroll 8
     for (int j = 0; j < m; j++) {
         double v = X[(size_t)j * S];
         if (pg.neg) v = -v;
@@ -105,14 +106,20 @@ __device__ __forceinline__ void blk_prdct(const BlkProg &pg, const BlkStep *__re
         double wn = Y[(size_t)(m - 1) * S] / bl;
         Dv[(size_t)(m - 1) * S] = dn;
         Wv[(size_t)(m - 1) * S] = wn;
-        for (int i0 = m - 2; i0 >= 1; i0 -= U) {
-            double yv[U], bv[U];
+        // rows m-2 .. 1 in chunks of U; the next chunk's loads are issued
+        // before this chunk's recurrence runs
+        double yv[U], bv[U], yn[U], bn[U];
+        auto load_e = [&](int i0, double *ya, double *ba) {
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int i = i0 - u;
-                yv[u] = (i >= 1) ? Y[(size_t)i * S] : 0.0;
-                bv[u] = (i >= 1) ? bm[(size_t)i * S] : 0.0;
+                ya[u] = (i >= 1) ? Y[(size_t)i * S] : 0.0;
+                ba[u] = (i >= 1) ? bm[(size_t)i * S] : 0.0;
             }
+        };
+        load_e(m - 2, yv, bv);
+        for (int i0 = m - 2; i0 >= 1; i0 -= U) {
+            load_e(i0 - U, yn, bn);
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int i = i0 - u;
@@ -124,6 +131,11 @@ __device__ __forceinline__ void blk_prdct(const BlkProg &pg, const BlkStep *__re
                     Wv[(size_t)i * S] = wn;
                 }
             }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                yv[u] = yn[u];
+                bv[u] = bn[u];
+            }
         }
         // row 1 (:222-228)
         const double den = bm[0] - rt - cm[0] * dn;
@@ -133,27 +145,39 @@ __device__ __forceinline__ void blk_prdct(const BlkProg &pg, const BlkStep *__re
         // Y = c W (:201-208)
         const int post = sp.post;
         const double c = sp.coef;
-        auto put = [&](int j, double v) {
+        const bool rd = post == BLK_AXPY;   // the update reads the pass's right-hand side
+        auto put = [&](int j, double v, double y) {
             if (post == BLK_COPY) Y[(size_t)j * S] = v;
-            else if (post == BLK_AXPY) Y[(size_t)j * S] = Y[(size_t)j * S] + c * v;
+            else if (post == BLK_AXPY) Y[(size_t)j * S] = y + c * v;
             else if (post == BLK_SCALE) Y[(size_t)j * S] = c * v;
         };
-        put(0, w);
-        for (int j0 = 1; j0 < m; j0 += U) {
-            double wv[U], dv[U];
+        put(0, w, rd ? Y[0] : 0.0);
+        double wv[U], dv[U], yw[U], wx[U], dx[U], yx[U];
+        auto load_f = [&](int j0, double *wa, double *da, double *ya) {
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int j = j0 + u;
-                wv[u] = (j < m) ? Wv[(size_t)j * S] : 0.0;
-                dv[u] = (j < m) ? Dv[(size_t)j * S] : 0.0;
+                wa[u] = (j < m) ? Wv[(size_t)j * S] : 0.0;
+                da[u] = (j < m) ? Dv[(size_t)j * S] : 0.0;
+                ya[u] = (rd && j < m) ? Y[(size_t)j * S] : 0.0;
             }
+        };
+        load_f(1, wv, dv, yw);
+        for (int j0 = 1; j0 < m; j0 += U) {
+            load_f(j0 + U, wx, dx, yx);
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int j = j0 + u;
                 if (j < m) {
                     w = wv[u] - dv[u] * w;
-                    put(j, w);
+                    put(j, w, yw[u]);
                 }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                wv[u] = wx[u];
+                dv[u] = dx[u];
+                yw[u] = yx[u];
             }
         }
     }

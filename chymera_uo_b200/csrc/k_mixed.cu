@@ -84,6 +84,8 @@ struct MixedDev {
     int *err;                   // error word
     int nit;                    // approximate solves (1 + corrections)
     int ntile;                  // MMA N = J rounded up to 64 (<= 256)
+    int probe_polls;            // test hook: > 0 makes every CTA first wait this many
+                                // polls on a barrier nothing arrives on (0: off)
 };
 
 struct MixedState {
@@ -92,6 +94,7 @@ struct MixedState {
     double *h_corr = nullptr;       // pinned [max_batch][L][8][2]
     size_t xbuf_bytes = 0;          // FP64 iterate (two or more corrections)
     int *h_err = nullptr;           // pinned
+    int probe_polls = 0;            // test hook (chy_dbg_mixed_probe)
     CUtensorMap tm_x{};             // X as rows of JMAX doubles: 16 x KMAX tiles, 128-byte swizzle
     CUtensorMap tm_xs{};            // the same with 16 x (KMAX-1) tiles: stores skip the boundary row
     bool tm_ok = false;
@@ -126,11 +129,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes));
 }
 
-// bounded wait on phase `parity`; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// bounded wait on phase `parity`; returns false after `limit` polls
+__device__ __forceinline__ bool mbar_wait_n(uint64_t *bar, uint32_t parity, long long limit)
 {
     const uint32_t a = smem_u32(bar);
-    for (long long i = 0; i < kSpinLimit; ++i) {
+    for (long long i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -143,6 +146,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     }
     return false;
 }
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) { return mbar_wait_n(bar, parity, kSpinLimit); }
 
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
@@ -485,21 +490,34 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     uint32_t ring_ph = 0, ring_pend = 0;   // residual ring slots: phase parity, copies in flight
     uint32_t ph_cv = 0;
     bool cv_pend = false;
+    bool mma_pend = false;   // a product's completion not yet observed
     bool failed = false;
 
     const long long items = (long long)nb * t.L;
-    if (tid == 0 && blockIdx.x < items) {
+    // test hook: a bounded wait on a barrier nothing arrives on (the sweep
+    // multipliers' barrier, before anything is issued on it), so the failure
+    // path runs with no copy or product in flight
+    if (x.probe_polls > 0) {
+        if (tid == 0 && !mbar_wait_n(bar_cv, 0, x.probe_polls)) *s_flag = 1;
+        __syncthreads();
+        failed = *s_flag != 0;
+    }
+    if (tid == 0 && blockIdx.x < items && !failed) {
         mbar_expect_tx(bar_a, kAImg);
         bulk_g2s(sA, x.aimg, kAImg, bar_a);   // U for the first transform
     }
-    bool a_inflight = blockIdx.x < items;
+    bool a_inflight = blockIdx.x < items && !failed;
+    long long fail_item = blockIdx.x;   // first item of this CTA left unsolved
 
+    // all threads wait; the phase advances only when every thread saw it
+    // complete, so after a failure the drain below waits on the same phase
     auto wait_all = [&](uint64_t *bar, uint32_t &ph) {
-        bool ok = mbar_wait(bar, ph);
-        ph ^= 1u;
+        const bool ok = mbar_wait(bar, ph);
         if (!ok) *s_flag = 1;
         __syncthreads();
-        return *s_flag == 0;
+        const bool good = *s_flag == 0;
+        if (good) ph ^= 1u;
+        return good;
     };
     // block sums of three per-thread values into d_red[0..2] (uniform call)
     auto block_sum3 = [&](double a, double b, double c) {
@@ -517,6 +535,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     };
 
     for (long long item = blockIdx.x; item < items && !failed; item += gridDim.x) {
+        fail_item = item;
         // mode-major order, modes l and l + N (same m) side by side and the
         // batch's solves innermost: the items in flight at once share a few
         // sweep-table slices, which then stay in L2
@@ -824,6 +843,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             if (a_inflight && !wait_all(bar_a, ph_a)) { failed = true; break; }
             a_inflight = false;
             if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma);
+            mma_pend = true;
             // the first chunk of pivot reciprocals is loaded while the product runs
             const float *swp = x.sw_piv + (size_t)m * NT * 128 + kq;   // row j at swp[j * 128]
             const int h = 32 * ((M + 63) / 64);   // M >= 63, h < M, h % 32 == 0
@@ -832,6 +852,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
 #pragma unroll
             for (int u = 0; u < 32; ++u) R[u] = swp[(size_t)((jh == 0 ? 0 : cl) + u) * 128];
             if (!wait_all(bar_mma, ph_mma)) { failed = true; break; }
+            mma_pend = false;
             tc_fence_after();
             float *cvs = reinterpret_cast<float *>(sBh);   // [j][p] multipliers for the back sweeps
             if (tid == 0) {
@@ -902,8 +923,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 tm_wait_st();
                 // the multipliers have landed (the barrier inside)
                 const bool cv_ok = wait_all(bar_cv, ph_cv);
-                cv_pend = false;
                 if (!cv_ok) { failed = true; break; }
+                cv_pend = false;
                 // meeting rows h-1 (top) and h (bottom):
                 // x_t = y'_t + (1-e_t) x_u, x_u = y''_u + (1-f_u) x_t
                 float xt, xu;
@@ -971,7 +992,9 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             if (!wait_all(bar_a, ph_a)) { failed = true; break; }
             a_inflight = false;
             if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma);
+            mma_pend = true;
             if (!wait_all(bar_mma, ph_mma)) { failed = true; break; }
+            mma_pend = false;
             tc_fence_after();
             const bool more = !last || item + gridDim.x < items;
             if (tid == 0 && more) {   // A tile free: U for the next transform
@@ -1100,12 +1123,30 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             }
         }
     }
-    // drain transfers still in flight (bounded), then release tensor memory
-    if (a_inflight && !failed) mbar_wait(bar_a, ph_a);
+    // drain copies and products still in flight (bounded), then release
+    // tensor memory
+    if (a_inflight) mbar_wait(bar_a, ph_a);
     for (int sl = 0; sl < kRingSlots; ++sl)
         if (ring_pend & (1u << sl)) mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u);
     if (cv_pend) mbar_wait(bar_cv, ph_cv);
-    if (failed && tid == 0) atomicExch(x.err, 1);
+    if (mma_pend) mbar_wait(bar_mma, ph_mma);
+    if (failed) {
+        // the modes this CTA left unsolved become NaN (interior of X), so the
+        // failure reaches PHI instead of passing silently; the error word
+        // tells the host
+        if (tid == 0) {
+            bulk_wait_all();
+            atomicExch(x.err, 1);
+        }
+        __syncthreads();
+        const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+        for (long long item = fail_item; item < items; item += gridDim.x) {
+            const int o = (int)(item / nb), b = (int)(item % nb);
+            const int l = (o & 1) ? (o >> 1) + t.N : (o >> 1);
+            double *Xl = w.X + (size_t)b * w.sX + (size_t)l * K * J;
+            for (int i = tid; i < NZ * M; i += blockDim.x) Xl[(size_t)(i / M) * J + i % M] = qnan;
+        }
+    }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
@@ -1279,6 +1320,7 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
 {
     *launches = 0;
     MixedDev d = p->mx->dev;
+    d.probe_polls = p->mx->probe_polls;
     d.nit = 1 + p->refine;
     if (d.nit > 8) d.nit = 8;
     if (d.nit > 2 && !d.xbuf) return CHY_ERR_NOT_SETUP;
@@ -1313,6 +1355,27 @@ int chy_mixed_collect(chy_plan *p, int nb)
     }
     if (cudaMemcpy(m.h_corr, m.dev.corr, sizeof(double) * m.dev.scorr * nb, cudaMemcpyDeviceToHost) != cudaSuccess)
         return CHY_ERR_CUDA;
+    return CHY_OK;
+}
+
+int chy_mixed_read_error(chy_plan *p, int *host_word, cudaStream_t s)
+{
+    if (p->precision != CHY_PREC_MIXED || !p->mx || !host_word) return CHY_OK;
+    if (cudaMemcpyAsync(host_word, p->mx->dev.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemsetAsync(p->mx->dev.err, 0, sizeof(int), s) != cudaSuccess)
+        return CHY_ERR_CUDA;
+    return CHY_OK;
+}
+
+int *chy_mixed_host_error_word(chy_plan *p)
+{
+    return (p->precision == CHY_PREC_MIXED && p->mx) ? p->mx->h_err : nullptr;
+}
+
+int chy_dbg_mixed_probe_set(chy_plan *p, int polls)
+{
+    if (p->precision != CHY_PREC_MIXED || !p->mx || polls < 0) return CHY_ERR_ARG;
+    p->mx->probe_polls = polls;
     return CHY_OK;
 }
 

@@ -97,6 +97,14 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches);
 // correction norms; CHY_ERR_TIMEOUT if a bounded wait expired.
 int chy_mixed_collect(chy_plan *p, int nb);
 void chy_mixed_fill_diag(const chy_plan *p, int slot, chy_diag *d);
+// Enqueues on s a copy of the device error word into *host_word (pinned)
+// and its reset; the word is non-zero after the stream is synchronised if a
+// bounded wait of an earlier mode solve expired.  No-op for other paths.
+int chy_mixed_read_error(chy_plan *p, int *host_word, cudaStream_t s);
+// The plan's own pinned error word (mixed plans), else null.
+int *chy_mixed_host_error_word(chy_plan *p);
+// Test hook behind chy_dbg_mixed_probe.
+int chy_dbg_mixed_probe_set(chy_plan *p, int polls);
 // Allocates the FP64 iterate used when two or more corrections are set.
 int chy_mixed_ensure_iterate(chy_plan *p);
 size_t chy_mixed_iterate_bytes(const chy_plan *p);

@@ -254,8 +254,14 @@ int chy_server::launch(SizeClass &c, Lane &ln)
         bp.rho[i] = dr;
         bp.phi[i] = df;
     }
-    const int st = chy_internal_run_batch(ln.plan, bp, nb, ln.stream);
+    int st = chy_internal_run_batch(ln.plan, bp, nb, ln.stream);
     if (st != CHY_OK) return st;
+    // the mode solve's error word, read back with the batch (checked at retirement)
+    if (int *ew = chy_mixed_host_error_word(ln.plan)) {
+        *ew = 0;
+        st = chy_mixed_read_error(ln.plan, ew, ln.stream);
+        if (st != CHY_OK) return st;
+    }
     for (int i = 0; i < nb; i++)
         if (copy_phi_write_set(ln.batch[i]->phi, bp.phi[i], c.J, c.K, c.L, ln.stream) != cudaSuccess)
             return CHY_ERR_CUDA;
@@ -316,7 +322,8 @@ void chy_server::run()
                 if (!ln.batch.empty()) {
                     const cudaError_t e = cudaEventQuery(ln.done);
                     if (e == cudaErrorNotReady) continue;
-                    retire(*kv.second, ln, e == cudaSuccess ? CHY_OK : CHY_ERR_CUDA);
+                    const int *ew = chy_mixed_host_error_word(ln.plan);
+                    retire(*kv.second, ln, e != cudaSuccess ? CHY_ERR_CUDA : (ew && *ew) ? CHY_ERR_TIMEOUT : CHY_OK);
                     progress = true;
                 }
         // admit waiting requests into idle lanes while their buffers fit

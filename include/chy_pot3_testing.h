@@ -44,6 +44,13 @@ long long chy_dbg_work(chy_plan *p, const char *name, double *out, long long cap
  * Returns a CHY_* status after synchronising the device. */
 int chy_dbg_umma(chy_plan *p, int which, const float *Bm_dev, float *D_dev, int nt);
 
+/* Failure-path hook of a CHY_PREC_MIXED plan: with polls > 0, every CTA of
+ * the plan's later mode solves first waits `polls` polls on a barrier that
+ * nothing arrives on, before it issues any copy or product; the wait runs
+ * out, the CTA poisons its modes with NaN, sets the device error word and
+ * exits, and the solve reports CHY_ERR_TIMEOUT.  0 switches it off. */
+int chy_dbg_mixed_probe(chy_plan *p, int polls);
+
 #ifdef __cplusplus
 }
 #endif
