@@ -238,21 +238,19 @@ def cpu_baseline(rhos, budget_s, max_solves):
 
 
 # ---------------------------------------------------------------- batched workload
-def run_batch_workload(args):
+def batched_record(steps, warmup, precisions=("mixed", "fp64", "blktri")):
     """64 seeded disks of uneven sizes (JMAX in {64,128,256}, KMAX in
     {32,64,128}, LMAX in {64,128,256}, random slope and H/r): one step = one
-    replay of a CUDA graph holding chy_solve_multi over all of them; the FP64
-    path is timed the same way.  One GPU (the rank-0 device)."""
+    replay of a CUDA graph holding chy_solve_multi over all of them, for each
+    mode-solve path.  Returns the record (device times, CUDA events)."""
     import torch
     import chymera_uo_b200 as chy
     from chymera_uo_b200 import synth
-    rank, local, ws = dist_info()
-    torch.cuda.set_device(local)
     n = 64
     dens = [synth.config_density(4, i) for i in range(n)]
     rhos = [chy.to_cuda_fortran(r) for r, _ in dens]
     res = {}
-    for prec in ("mixed", "fp64"):
+    for prec in precisions:
         cache = {}
         plans = []
         for _, g in dens:
@@ -266,39 +264,58 @@ def run_batch_workload(args):
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
             chy.solve_multi(plans, rhos, outs)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             graph.replay()
         torch.cuda.synchronize()
-        launches0 = sum(p.launches for p in cache.values())
+        k = steps if prec != "blktri" else max(3, steps // 4)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(torch.cuda.current_device()) as clk:
             e0.record()
-            for _ in range(args.steps):
+            for _ in range(k):
                 graph.replay()
             e1.record()
             torch.cuda.synchronize()
-        res[prec] = {"ms": e0.elapsed_time(e1), "outs": outs, "clocks": clk.summary(),
-                     "sizes": len(cache), "plans": cache}
-        del graph
-    worst = 0.0
-    for (_, g), a, b in zip(dens, res["mixed"]["outs"], res["fp64"]["outs"]):
-        sl = (slice(0, g.jmax + 1), slice(0, g.kmax + 1))
-        worst = max(worst, float(torch.linalg.vector_norm(a[sl] - b[sl]) / torch.linalg.vector_norm(b[sl])))
-    ms = res["mixed"]["ms"]
-    value = n * args.steps / (ms * 1e-3)
-    line = {"metric": "pot3 solves/s, 64 uneven grids per CUDA-graph replay (mixed vs FP64)", "value": value,
-            "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "mixed: f16 hi/lo tensor-core + f32 + f64", "data": "synthetic",
-            "config": {"workload": "batched: 64 seeded disks, JMAX {64,128,256} x KMAX {32,64,128} x "
-                                   "LMAX {64,128,256}, slope U[-2,-1], H/r U[0.03,0.1]",
-                       "distinct_grids": res["mixed"]["sizes"], "solves_per_step": n,
-                       "launch": "one CUDA graph replay of chy_solve_multi per step",
-                       "l2": "inputs larger than L2 (all 64 densities resident)"},
-            "fp64_gpu": {"value": n * args.steps / (res["fp64"]["ms"] * 1e-3), "unit": UNIT,
-                         "ms_per_step": res["fp64"]["ms"] / args.steps},
-            "accuracy": {"rel_l2_mixed_vs_fp64_max": worst},
-            "clocks": res["mixed"]["clocks"]}
+        ms = e0.elapsed_time(e1) / k
+        res[prec] = {"ms": ms, "outs": outs, "clocks": clk.summary(), "sizes": len(cache),
+                     "value": n / (ms * 1e-3), "steps": k}
+        del graph, cache, plans
+    worst = {}
+    base = "blktri" if "blktri" in res else "fp64"
+    for prec in res:
+        if prec == base:
+            continue
+        w = 0.0
+        for (_, g), a, b in zip(dens, res[prec]["outs"], res[base]["outs"]):
+            sl = (slice(0, g.jmax + 1), slice(0, g.kmax + 1))
+            w = max(w, float(torch.linalg.vector_norm(a[sl] - b[sl]) / torch.linalg.vector_norm(b[sl])))
+        worst[f"rel_l2_{prec}_vs_{base}_max"] = w
+    rec = {"metric": "pot3 solves/s, 64 uneven grids per CUDA-graph replay", "unit": UNIT,
+           "value": res["mixed"]["value"] if "mixed" in res else None,
+           "per_precision": {p: {"value": r["value"], "ms_per_step": r["ms"], "steps": r["steps"]}
+                             for p, r in res.items()},
+           "config": {"workload": "batched: 64 seeded disks, JMAX {64,128,256} x KMAX {32,64,128} x "
+                                  "LMAX {64,128,256}, slope U[-2,-1], H/r U[0.03,0.1]",
+                      "distinct_grids": next(iter(res.values()))["sizes"], "solves_per_step": n,
+                      "launch": "one CUDA graph replay of chy_solve_multi per step (grids on side streams)",
+                      "l2": "inputs larger than L2 (all 64 densities resident)"},
+           "accuracy": worst, "clocks": res[precisions[0]]["clocks"]}
+    for p in res:
+        if p != "mixed" and "mixed" in res:
+            rec[f"mixed_over_{p}"] = res["mixed"]["value"] / res[p]["value"]
+    return rec
+
+
+def run_batch_workload(args):
+    """The batched workload alone (one GPU, the rank-0 device)."""
+    import torch
+    rank, local, ws = dist_info()
+    torch.cuda.set_device(local)
+    rec = batched_record(args.steps, args.warmup)
+    line = {"metric": rec["metric"] + " (mixed vs FP64)", "value": rec["value"], "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": rec["per_precision"]["mixed"]["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed: f16 hi/lo tensor-core + f32 + f64", "data": "synthetic", "config": rec["config"],
+            "per_precision": rec["per_precision"], "accuracy": rec["accuracy"], "clocks": rec["clocks"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -408,17 +425,15 @@ def run_step_workload(args):
 
 
 # ---------------------------------------------------------------- serving workload
-def run_serving_workload(args):
-    """Poisson request streams (mean rates --rates) of seeded disks with the
-    serving mix of grid sizes (20% 512x128x512, the rest drawn from the batched
-    size set) through chy_server; reports solves/s and p50/p99 latency per rate
-    for the mixed-precision server and the plain FP64 server."""
+def serving_record(rates, max_requests, seconds_per_rate, precisions=("mixed", "fp64")):
+    """Poisson request streams at each mean rate in `rates` of seeded disks
+    with the serving mix of grid sizes (20% 512x128x512, the rest drawn from
+    the batched size set) through chy_server: min(max_requests, rate x
+    seconds_per_rate) requests per rate.  Reports solves/s and p50/p99
+    latency per rate for each precision."""
     import threading
-    import torch
     import chymera_uo_b200 as chy
     from chymera_uo_b200 import synth
-    rank, local, ws = dist_info()
-    torch.cuda.set_device(local)
     # a pool of distinct requests, reused round robin (a pool entry is
     # resubmitted only after its previous request finished)
     pool_n = 48
@@ -430,16 +445,16 @@ def run_serving_workload(args):
         f = chy.pinned_fortran(rho.shape)
         f[...] = 0.0
         pool.append(((g.jmax, g.kmax, g.lmax), a, f))
-    rates = [float(r) for r in args.rates.split(",") if r]
+    big = sum(1 for k, _, _ in pool if k == (512, 128, 512))
     out = []
-    for prec in ("mixed", "fp64"):
+    for prec in precisions:
         srv = chy.Server(prec, hbm_budget=96 << 30, max_batch=4)
         grids = {k: chy.grid(*k) for k, _, _ in pool}
         # warm every size class once (plans are created on first use)
         for t in [srv.submit(grids[k], a, f) for k, a, f in pool]:
             srv.wait(t)
         for rate in rates:
-            n = args.requests
+            n = int(min(max_requests, max(pool_n, round(rate * seconds_per_rate))))
             rng = np.random.default_rng(int(rate))
             gaps = rng.exponential(1.0 / rate, n)
             tickets = [None] * n
@@ -473,24 +488,75 @@ def run_serving_workload(args):
                     lat[last[j]] = srv.wait(tickets[last[j]])
             wall = time.perf_counter() - t_start
             st1 = srv.stats()
-            out.append({"precision": prec, "rate_req_s": rate, "requests": n, "solves_per_s": n / wall,
-                        "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                        "batches": st1["batches"] - st0["batches"]})
+            out.append({"precision": prec, "rate_req_s": rate, "requests": n, "wall_s": wall,
+                        "solves_per_s": n / wall, "p50_ms": float(np.percentile(lat, 50)),
+                        "p99_ms": float(np.percentile(lat, 99)), "batches": st1["batches"] - st0["batches"]})
         srv.close()
-    line = {"metric": "pot3 serving: solves/s and p50/p99 latency vs Poisson arrival rate (mixed vs FP64)",
-            "value": max(r["solves_per_s"] for r in out if r["precision"] == "mixed"), "unit": UNIT,
-            "n_gpus": ws, "higher_is_better": True, "data": "synthetic",
-            "config": {"workload": "serving: seeded disks, 20% 512x128x512, 80% from the batched size set; "
-                                   f"{pool_n} distinct requests reused round robin; pinned host buffers; "
-                                   "latency = submit to completion on the host clock",
-                       "server": "chy_server, max_batch 4, two lanes per grid"},
+    return {"metric": "pot3 serving: solves/s and p50/p99 latency vs Poisson arrival rate", "unit": UNIT,
+            "value": max(r["solves_per_s"] for r in out if r["precision"] == precisions[0]),
+            "config": {"workload": f"serving: seeded disks, 20% 512x128x512 ({big} of {pool_n} pool entries), "
+                                   "80% from the batched size set; min(10000, rate x "
+                                   f"{seconds_per_rate:g} s) requests per rate; {pool_n} distinct requests "
+                                   "reused round robin; pinned host buffers; latency = submit to completion "
+                                   "on the host clock",
+                       "server": "chy_server, max_batch 4, two lanes per grid",
+                       "precisions": list(precisions)},
             "per_rate": out}
+
+
+def run_serving_workload(args):
+    """The serving workload alone (one GPU, the rank-0 device)."""
+    import torch
+    rank, local, ws = dist_info()
+    torch.cuda.set_device(local)
+    rates = [float(r) for r in args.rates.split(",") if r]
+    rec = serving_record(rates, args.requests, args.serve_seconds)
+    line = {"metric": rec["metric"] + " (mixed vs FP64)", "value": rec["value"], "unit": UNIT, "n_gpus": ws,
+            "higher_is_better": True, "data": "synthetic", "config": rec["config"], "per_rate": rec["per_rate"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
 
 
 # ---------------------------------------------------------------- GPU arm
+def pcie_ceiling(nbytes=512 << 20, reps=5):
+    """Pinned host <-> device copy bandwidth of this box (GB/s, CUDA events):
+    each direction alone and both at once on two streams."""
+    import torch
+    h_in = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h_out = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d_in = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d_out = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(fn, stream):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        return e0, e1
+
+    with torch.cuda.stream(s1):
+        d_in.copy_(h_in, non_blocking=True)
+        h_out.copy_(d_out, non_blocking=True)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s1):
+        a = timed(lambda: d_in.copy_(h_in, non_blocking=True), s1)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s1):
+        b = timed(lambda: h_out.copy_(d_out, non_blocking=True), s1)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s1):
+        c = timed(lambda: d_in.copy_(h_in, non_blocking=True), s1)
+    with torch.cuda.stream(s2):
+        d = timed(lambda: h_out.copy_(d_out, non_blocking=True), s2)
+    torch.cuda.synchronize()
+    gbs = lambda ev: reps * nbytes / (ev[0].elapsed_time(ev[1]) * 1e-3) / 1e9
+    return {"h2d": gbs(a), "d2h": gbs(b), "concurrent_h2d": gbs(c), "concurrent_d2h": gbs(d),
+            "bytes_per_copy": nbytes}
+
+
 def rel_l2(a, b):
     return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
 
@@ -512,8 +578,12 @@ def main():
                     help="pot3: 256x128x256 mixed (default); batch: 64 uneven grids from one captured "
                          "graph; serving: Poisson request stream with p50/p99 latency; step: one time "
                          "step's gravity (solve, star potential, SOURCE terms)")
-    ap.add_argument("--rates", default="200,1000,5000", help="serving: mean arrival rates (req/s)")
-    ap.add_argument("--requests", type=int, default=400, help="serving: requests per rate")
+    ap.add_argument("--rates", default="100,300,1000,3000,5000", help="serving: mean arrival rates (req/s)")
+    ap.add_argument("--requests", type=int, default=10000, help="serving: most requests per rate")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="serving: requests per rate are min(--requests, rate x this)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="pot3 workload: skip the batched and serving records appended after the timed region")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -548,7 +618,9 @@ def main():
     plan = chy.Plan(g, args.precision, B)
     if args.precision == "mixed":
         plan.set_refine(args.refine)
-    plan64 = chy.Plan(g, "fp64", B)
+    plan64 = chy.Plan(g, "fp64", B)          # FP64 eigenbasis mode solve
+    planbk = chy.Plan(g, "blktri", B)        # FP64 in BLKTRI's order: the plain FP64 pot3
+    eig_phis = [chy.fortran_zeros_cuda((J + 2, K + 2, L)) for _ in range(B)]
     stream = torch.cuda.current_stream()
 
     # ---- device-resident throughput (the `value`)
@@ -585,29 +657,42 @@ def main():
                 "algorithmic_bytes": alg, "launch_ms": mode_ms,
                 "stage_ms_per_step": {k: v / max(calls, 1) for k, v in stage.items()}}
 
-    # ---- plain FP64 GPU path on the same inputs (same step shape)
-    for _ in range(args.warmup):
-        plan64.solve_batch(rhos, ref_phis)
-    barrier()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    k64 = max(3, args.steps // 2)
-    f0.record(stream)
-    for _ in range(k64):
-        plan64.solve_batch(rhos, ref_phis)
-    f1.record(stream)
-    barrier()
-    ms64 = max_over_ranks(f0.elapsed_time(f1))
-    fp64_value = ws * B * k64 / (ms64 * 1e-3)
+    # ---- the FP64 GPU paths on the same inputs (same step shape): BLKTRI's
+    # order (the plain FP64 pot3, the reference's rounding) and the eigenbasis
+    def time_path(pl, outs, k):
+        for _ in range(args.warmup):
+            pl.solve_batch(rhos, outs)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(k):
+            pl.solve_batch(rhos, outs)
+        f1.record(stream)
+        barrier()
+        m = max_over_ranks(f0.elapsed_time(f1))
+        return ws * B * k / (m * 1e-3), m / k, k
 
-    # ---- accuracy: mixed vs the FP64 GPU path, device status words
+    bk_value, bk_ms, bk_k = time_path(planbk, ref_phis, 3)
+    eig_value, eig_ms, eig_k = time_path(plan64, eig_phis, max(3, args.steps // 2))
+
+    # ---- accuracy: mixed and the eigenbasis path vs the BLKTRI-order FP64
+    # path, device status words
     _, diags = plan.solve_batch(rhos, phis, diag=True)
     torch.cuda.synchronize()
-    errs, maxe = [], []
-    for a, b in zip(phis, ref_phis):
-        d = (a[: J + 1, : K + 1] - b[: J + 1, : K + 1])
-        errs.append(float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(b[: J + 1, : K + 1])))
-        maxe.append(float(d.abs().max() / b[: J + 1, : K + 1].abs().max()))
-    accuracy = {"rel_l2_vs_fp64_gpu_max": max(errs), "max_rel_vs_fp64_gpu": max(maxe),
+
+    def worst(xs, ys):
+        errs, maxe = [], []
+        for a, b in zip(xs, ys):
+            d = (a[: J + 1, : K + 1] - b[: J + 1, : K + 1])
+            errs.append(float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(b[: J + 1, : K + 1])))
+            maxe.append(float(d.abs().max() / b[: J + 1, : K + 1].abs().max()))
+        return max(errs), max(maxe)
+
+    e_mx, m_mx = worst(phis, ref_phis)
+    e_eg, _ = worst(eig_phis, ref_phis)
+    accuracy = {"rel_l2_vs_fp64_gpu_max": e_mx, "max_rel_vs_fp64_gpu": m_mx,
+                "fp64_gpu_reference": "BLKTRI-order FP64 path (CHY_PREC_FP64_BLKTRI)",
+                "rel_l2_fp64_eigen_vs_blktri_max": e_eg,
                 "corr_rel_solve0": diags[0]["corr_rel"], "solves_checked": B}
 
     # ---- single-solve latency (device-resident, one launch sequence each)
@@ -636,7 +721,7 @@ def main():
         a[...] = b
     for a in pin_p:
         a[...] = 0.0
-    h2d = B * 8 * (J + 2) * (K + 2) * L                      # RHO
+    h2d = B * 8 * (J + 2) * (K - 1) * L                      # RHO rows K = 2..KMAX (the read set's rows)
     d2h = B * 8 * L * (K * (J + 2) + (J + 1))                # PHI's write set
     ke = max(3, args.steps // 4)
     for _ in range(args.warmup):
@@ -653,6 +738,11 @@ def main():
     e2e = {"value": ws * B * ke / (mse * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "steps": ke,
            "api": "chy_solve_batch with CHY_PTR_HOST (pinned numpy buffers)"}
+    pcie = pcie_ceiling()
+    e2e["pcie_gbs"] = pcie
+    e2e["achieved_gbs"] = {"h2d": h2d * ke / (mse * 1e-3) / 1e9, "d2h": d2h * ke / (mse * 1e-3) / 1e9}
+    e2e["pcie_frac"] = max(e2e["achieved_gbs"]["h2d"] / pcie["concurrent_h2d"],
+                           e2e["achieved_gbs"]["d2h"] / pcie["concurrent_d2h"])
     host_ok = np.array_equal(pin_p[0], phis[0].cpu().numpy())
     accuracy["host_path_equals_device_path"] = bool(host_ok)
 
@@ -663,8 +753,10 @@ def main():
         ws_sl = (slice(0, J + 1), slice(0, K + 1))
         got = [p.cpu().numpy() for p in phis[: len(outs)]]
         g64 = [p.cpu().numpy() for p in ref_phis[: len(outs)]]
+        geg = [p.cpu().numpy() for p in eig_phis[: len(outs)]]
         accuracy["rel_l2_mixed_vs_oracle_max"] = max(rel_l2(a[ws_sl], b[ws_sl]) for a, b in zip(got, outs))
         accuracy["rel_l2_fp64_vs_oracle_max"] = max(rel_l2(a[ws_sl], b[ws_sl]) for a, b in zip(g64, outs))
+        accuracy["rel_l2_fp64_eigen_vs_oracle_max"] = max(rel_l2(a[ws_sl], b[ws_sl]) for a, b in zip(geg, outs))
         accuracy["oracle_solves_compared"] = len(outs)
 
     if rank == 0:
@@ -680,9 +772,21 @@ def main():
                                  "RHO + PHI resident)"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
                 "clocks": clocks, "latency_ms": latency,
-                "fp64_gpu": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms64 / k64,
-                             "mixed_over_fp64": value / fp64_value},
+                "fp64_gpu": {"value": bk_value, "unit": UNIT, "ms_per_step": bk_ms, "steps": bk_k,
+                             "path": "plain FP64 pot3: BLKTRI generalized cyclic reduction in the "
+                                     "reference's order (CHY_PREC_FP64_BLKTRI)",
+                             "mixed_over_fp64": value / bk_value,
+                             "eigen": {"value": eig_value, "unit": UNIT, "ms_per_step": eig_ms, "steps": eig_k,
+                                       "path": "FP64 eigenbasis + radial Thomas (CHY_PREC_FP64)",
+                                       "mixed_over_eigen": value / eig_value}},
                 "accuracy": accuracy}
+        if ws == 1 and not args.no_extra:
+            # configs 4 and 5, after the timed region
+            del plan64, planbk
+            torch.cuda.empty_cache()
+            line["batched"] = batched_record(5, 3)
+            line["serving"] = serving_record([float(r) for r in args.rates.split(",") if r], args.requests,
+                                             args.serve_seconds)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

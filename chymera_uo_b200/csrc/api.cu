@@ -58,6 +58,18 @@ struct Packer {
 
 static int ensure_host_staging(chy_plan *p);
 
+// The plan's arrays live on the device that was current at chy_plan_create;
+// launching with another device current would hand them to the wrong GPU.
+static int check_device(const chy_plan *p)
+{
+    int dev = -1;
+    CHY_CUDA(cudaGetDevice(&dev));
+    if (dev != p->device)
+        return fail(CHY_ERR_ARG, "plan was created on device " + std::to_string(p->device) + ", device " +
+                                     std::to_string(dev) + " is current");
+    return CHY_OK;
+}
+
 extern "C" {
 
 void chy_grid_defaults(chy_grid *g, int jmax, int kmax, int lmax)
@@ -163,6 +175,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
         delete p;
         return cuda_fail(ce, "cudaGetDevice");
     }
+    p->device = dev;
 
     // ---- tables
     Packer pk;
@@ -580,6 +593,10 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
     const HostPlan &hp = p->hp;
     for (int i = 0; i < n; i++)
         if (!rho[i] || !phi[i]) return fail(CHY_ERR_ARG, "null rho/phi pointer");
+    if (n > 0) {
+        const int dst = check_device(p);
+        if (dst != CHY_OK) return dst;
+    }
     if (ptr_kind == CHY_PTR_DEVICE) {
         for (int first = 0; first < n;) {
             const int nb = std::min(std::min(n - first, p->max_batch), kMaxBatchPtrs);
@@ -600,7 +617,6 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
     // Three-stage pipeline over chunks of stage_chunk solves: copy in on
     // s_h2d, solve on the caller's stream, copy out on s_d2h.  A slot is
     // reused only after its previous copy out has finished.
-    const size_t vb = p->nvol * sizeof(double);
     // with a host COEF destination, one solve per chunk (COEF is per solve)
     const int c = p->coef_host ? 1 : p->stage_chunk, R = chy_plan::kStageSlots;
     bool used[chy_plan::kStageSlots] = {};
@@ -614,7 +630,8 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         for (int i = 0; i < nb; i++) {
             double *dr = base + (size_t)i * 2 * p->nvol, *df = dr + p->nvol;
             const double *hr = rho[first + i];
-            CHY_CUDA(cudaMemcpyAsync(dr, hr, vb, cudaMemcpyHostToDevice, p->s_h2d));
+            CHY_CUDA(copy_rho_read_set(dr, hr, hp.J, hp.K, hp.L, p->star.on && p->star.indirect ? hp.K : hp.K - 1,
+                                       p->s_h2d));
             // the external potential updates the cells the solve leaves
             // alone: start them from the caller's values
             if (p->star.on)
@@ -710,6 +727,8 @@ extern "C" int chy_solve_multi(int n, chy_plan *const *plans, const double *cons
     std::vector<std::vector<int>> members;
     for (int i = 0; i < n; i++) {
         if (!plans[i] || !rho[i] || !phi[i]) return fail(CHY_ERR_ARG, "null plan or buffer in request list");
+        const int dst = check_device(plans[i]);
+        if (dst != CHY_OK) return dst;
         size_t g = 0;
         while (g < order.size() && order[g] != plans[i]) g++;
         if (g == order.size()) {
@@ -835,10 +854,15 @@ extern "C" int chy_solve_static(chy_plan *p, const double *rho, double *phi, voi
     int dev = 0;
     CHY_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return fail(CHY_ERR_ARG, "device ordinal out of range");
+    if (dev != p->device)
+        return fail(CHY_ERR_ARG, "chy_solve_static: plan was created on device " + std::to_string(p->device) +
+                                     ", device " + std::to_string(dev) + " is current");
     double *base = nullptr;
     {
         // first call on each device (with that device current): look the
-        // array up once; later calls reuse the address
+        // array up once; later calls reuse the address, which stays valid
+        // for the life of the process's context on that device (a
+        // cudaDeviceReset would invalidate it)
         std::lock_guard<std::mutex> lk(g_static_mu);
         if (!g_static_ptr[dev]) {
             void *ptr = nullptr;
@@ -872,6 +896,7 @@ extern "C" int chy_solve_static(chy_plan *p, const double *rho, double *phi, voi
     CHY_CUDA(launch_solve_fp64(t, w, 1, p->num_sms, s));
     int nv = 0;
     CHY_CUDA(launch_inverse(t, bp, w, StarDev{}, 1, s, &nv));   // POT3 alone
+    p->launches += 1 + 2 + 1 + 3 + nv;
     return CHY_OK;
 }
 

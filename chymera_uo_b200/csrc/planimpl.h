@@ -21,6 +21,7 @@ struct chy_plan {
     int max_batch = 1;
     int refine = 1;
     int num_sms = 148;
+    int device = 0;                // the device the plan's tables and work space live on
     char *d_tables = nullptr;
     size_t table_bytes = 0;
     char *d_work = nullptr;
@@ -65,6 +66,18 @@ inline cudaError_t copy_phi_write_set(double *host, const double *dev, int J, in
                                       cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) return e;
     return cudaMemcpy2DAsync(host, plane, dev, plane, ((size_t)J + 1) * sizeof(double), L, cudaMemcpyDeviceToHost, s);
+}
+
+// Copies the rows of RHO a solve reads, RHO(:, 2:nrows+1, :), from the
+// caller's host array to a device copy of the whole volume; the other rows of
+// the device copy are never read.  A solve reads RHO(2:JMAX, 2:KMAX, :)
+// (nrows = KMAX-1); the INDIRECT star shift also reads row KMAX+1 (nrows = KMAX).
+inline cudaError_t copy_rho_read_set(double *dev, const double *host, int J, int K, int L, int nrows,
+                                     cudaStream_t s)
+{
+    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2, plane = J2 * K2 * sizeof(double);
+    return cudaMemcpy2DAsync(dev + J2, plane, host + J2, plane, (size_t)nrows * J2 * sizeof(double), L,
+                             cudaMemcpyHostToDevice, s);
 }
 
 // Copies the cells of PHI that a solve never writes, PHI(:, KMAX+2, :) and

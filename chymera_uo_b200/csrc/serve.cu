@@ -244,13 +244,12 @@ int chy_server::make_class(Request *rq, SizeClass **out)
 // Copies in, solves and copies out the lane's batch on its stream.
 int chy_server::launch(SizeClass &c, Lane &ln)
 {
-    const size_t vb = c.nvol * sizeof(double);
     BatchPtrs bp{};
     const int nb = (int)ln.batch.size();
     for (int i = 0; i < nb; i++) {
         Request *rq = ln.batch[i];
         double *dr = reinterpret_cast<double *>(arena_base + rq->buf_off), *df = dr + c.nvol;
-        if (cudaMemcpyAsync(dr, rq->rho, vb, cudaMemcpyHostToDevice, ln.stream) != cudaSuccess) return CHY_ERR_CUDA;
+        if (copy_rho_read_set(dr, rq->rho, c.J, c.K, c.L, c.K - 1, ln.stream) != cudaSuccess) return CHY_ERR_CUDA;
         bp.rho[i] = dr;
         bp.phi[i] = df;
     }

@@ -107,6 +107,10 @@ void chy_grid_defaults(chy_grid *g, int jmax, int kmax, int lmax);
 int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **out);
 void chy_plan_destroy(chy_plan *p);
 
+/* Every solve entry point needs the device that was current at
+ * chy_plan_create to be current when it is called; otherwise it returns
+ * CHY_ERR_ARG. */
+
 /* One solve: BDYGEN(MAXTRM,ISYM,REDGE) then POT3(NPOINT,IPRINT=0).
  * rho/phi are device pointers (CHY_PTR_DEVICE) or host pointers
  * (CHY_PTR_HOST; pinned memory gives full copy bandwidth).  stream may be
@@ -279,9 +283,11 @@ long long chy_plan_launch_count(const chy_plan *p);
  * CHY_ERR_UNSUPPORTED.  The array is cleared (cudaMemsetAsync) at the
  * start of every call.  The first call on each device looks the array up
  * (cudaGetSymbolAddress) with that device current; make it before any
- * stream capture starts.  All calls on one device share the array, so calls
- * that overlap in time (several streams or threads) race: serialise them.
- * Asynchronous on `stream` like chy_solve. */
+ * stream capture starts.  The address is kept for the process's life, so a
+ * cudaDeviceReset in between is not supported.  All calls on one device share
+ * the array, so calls that overlap in time (several streams or threads) race:
+ * serialise them.  The plan's device must be current (CHY_ERR_ARG
+ * otherwise).  Asynchronous on `stream` like chy_solve. */
 int chy_solve_static(chy_plan *p, const double *rho, double *phi, void *stream);
 
 #ifdef __cplusplus
