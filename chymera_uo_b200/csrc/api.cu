@@ -152,7 +152,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     }
     if (precision == CHY_PREC_MIXED && !chy_mixed_supported(&p->hp)) {
         delete p;
-        return fail(CHY_ERR_UNSUPPORTED, "mixed precision needs KMAX <= 128 and JMAX a multiple of 16 in 64..256");
+        return fail(CHY_ERR_UNSUPPORTED, "mixed precision needs KMAX <= 128 and JMAX in 64..1024 (or a multiple of 16 up to 256)");
     }
     p->precision = precision;
     p->max_batch = max_batch;
@@ -199,7 +199,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
         o_bsg = pk.vec(bs.stages);
         o_bmt = pk.vec(blk_bm_table(hp));
     }
-    size_t o_ext = chy_mixed_pack_tables(&hp, &pk.host);
+    size_t o_ext = chy_mixed_pack_tables(&hp, &pk.host, precision == CHY_PREC_MIXED);
     p->table_bytes = pk.host.size();
     ce = cudaMalloc(&p->d_tables, p->table_bytes);
     if (ce == cudaSuccess) ce = cudaMemcpy(p->d_tables, pk.host.data(), p->table_bytes, cudaMemcpyHostToDevice);

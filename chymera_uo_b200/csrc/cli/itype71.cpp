@@ -2,7 +2,7 @@
 // on libchy_pot3.
 //
 //   chy_itype71 [--dir D] [--jmax J --kmax K --lmax L] [--hj HJ --hk HK]
-//               [--precision fp64|mixed] [--literal gcc|r8] [--check-input]
+//               [--precision blktri|fp64|mixed] [--literal gcc|r8] [--check-input]
 //
 // Reads D/fort.5 (radhydro/io.f:100-119: ITYPE must be 71; ITSTOP names the
 // output) and D/fort.2 (io.f:157-166, list-directed: PINDEX, CON2, RRR2,
@@ -106,7 +106,7 @@ bool write_record(std::FILE *f, const void *data, size_t bytes)
 int main(int argc, char **argv)
 {
     std::string dir = ".";
-    int J = 256, K = 128, L = 256, HJ = 256, HK = 256, precision = CHY_PREC_FP64, literal = CHY_LITERAL_GCC;
+    int J = 256, K = 128, L = 256, HJ = 256, HK = 256, precision = CHY_PREC_FP64_BLKTRI, literal = CHY_LITERAL_GCC;
     bool check = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
@@ -123,7 +123,10 @@ int main(int argc, char **argv)
         else if (a == "--lmax") L = std::atoi(val("--lmax"));
         else if (a == "--hj") HJ = std::atoi(val("--hj"));
         else if (a == "--hk") HK = std::atoi(val("--hk"));
-        else if (a == "--precision") precision = std::string(val("--precision")) == "mixed" ? CHY_PREC_MIXED : CHY_PREC_FP64;
+        else if (a == "--precision") {
+            const std::string v = val("--precision");
+            precision = v == "mixed" ? CHY_PREC_MIXED : v == "fp64" ? CHY_PREC_FP64 : CHY_PREC_FP64_BLKTRI;
+        }
         else if (a == "--literal") literal = std::string(val("--literal")) == "r8" ? CHY_LITERAL_R8 : CHY_LITERAL_GCC;
         else if (a == "--check-input") check = true;
         else {

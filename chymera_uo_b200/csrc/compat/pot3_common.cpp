@@ -14,7 +14,9 @@
 //
 // Compile-time sizes (required): -DCHY_JMAX=.. -DCHY_KMAX=.. -DCHY_LMAX=..
 // Options: -DCHY_PARTICLE=1 solves for RHOTOT (pot/pot3.f:74-78);
-//          -DCHY_PRECISION=1 uses the mixed-precision tensor-core path;
+//          -DCHY_PRECISION selects the mode solve: 2 (default) BLKTRI in the
+//          reference's order, 0 the FP64 eigenbasis solver, 1 the
+//          mixed-precision tensor-core path;
 //          -DCHY_LITERAL_KIND=1 for -r8 / -fdefault-real-8 builds.
 //
 // Semantics.  SETBDY records that the boundary tables may be built (the
@@ -43,7 +45,7 @@
 #define CHY_PARTICLE 0
 #endif
 #ifndef CHY_PRECISION
-#define CHY_PRECISION CHY_PREC_FP64
+#define CHY_PRECISION CHY_PREC_FP64_BLKTRI
 #endif
 #ifndef CHY_LITERAL_KIND
 #define CHY_LITERAL_KIND CHY_LITERAL_GCC

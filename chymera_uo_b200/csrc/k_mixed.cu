@@ -88,6 +88,19 @@ struct MixedDev {
                                 // polls on a barrier nothing arrives on (0: off)
 };
 
+// Arrays of the multi-kernel mixed pipeline (grids with JMAX > 256 or JMAX
+// not a multiple of 16).  item = solve * L + mode; Jt = JMAX rounded up to a
+// multiple of 256 (the GEMM N tile).
+struct WideDev {
+    double *xit;                // [item][K][J] FP64 iterate
+    size_t sxit;
+    float *R;                   // [item][Jt][128] FP32: residual rows, then the sweep results
+    float *O;                   // [item][Jt][128] FP32: products U r (W) and V w (delta)
+    size_t sro;
+    unsigned *rmax, *wmax;      // [item][Jt/256] bits of max |r| and max |w| per tile
+    int Jt, nt;                 // nt = Jt / 256
+};
+
 struct MixedState {
     size_t o_aimg = 0, o_lam = 0;   // offsets into the packed table image
     MixedDev dev{};
@@ -95,6 +108,8 @@ struct MixedState {
     size_t xbuf_bytes = 0;          // FP64 iterate (two or more corrections)
     int *h_err = nullptr;           // pinned
     int probe_polls = 0;            // test hook (chy_dbg_mixed_probe)
+    WideDev wide{};                 // the multi-kernel pipeline of grids k_mode_mixed does not cover
+    bool is_wide = false;
     CUtensorMap tm_x{};             // X as rows of JMAX doubles: 16 x KMAX tiles, 128-byte swizzle
     CUtensorMap tm_xs{};            // the same with 16 x (KMAX-1) tiles: stores skip the boundary row
     bool tm_ok = false;
@@ -1153,13 +1168,286 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
 }
 
 // ---------------------------------------------------------------------------
+// Wide pipeline: grids whose radial extent does not fit one CTA's tiles
+// (JMAX > 256, e.g. the 512 x 128 x 512 serving class) or whose rows are not
+// 16-byte tiles (JMAX not a multiple of 16).  The same refinement as
+// k_mode_mixed -- FP64 residual, FP16 hi/lo tensor-core transforms with FP32
+// accumulation, FP32 radial sweeps from the same sweep table, FP64 update --
+// as five kernels per approximate solve, with the intermediate FP32 arrays in
+// device memory:
+//   k_wide_resid   r = Y - A x (FP64) -> R[item][j][k] (FP32), per-tile max |r|
+//   k_wide_gemm    W = U r: one CTA per (item, 256-column tile), tcgen05
+//   k_wide_sweep   (T_r(m) + lam_p) w = W_p, one thread per (item, p) -> R
+//   k_wide_gemm    delta = V w
+//   k_wide_update  x += delta (FP64); the last solve writes X's interior
+// ---------------------------------------------------------------------------
+constexpr int kWideN = 256;      // GEMM N tile (radial columns)
+constexpr int kWideMaxJ = 1024;  // largest JMAX of the wide pipeline
+constexpr int kWideTiles = kWideMaxJ / kWideN;
+
+template <bool kFirst>
+__global__ void __launch_bounds__(256) k_wide_resid(DevTables t, Work w, WideDev d, int nb)
+{
+    __shared__ float tile[32][129];
+    __shared__ float red[8];
+    const int item = blockIdx.y, b = item / t.L, l = item % t.L, j0 = blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, j = j0 + tx;
+    const int M = t.M, NZ = t.NZ, J = t.J;
+    const int m = l <= t.N ? l : l - t.N;
+    const double xl2 = 2.0 * (t.xlamm[m] - 1.0);
+    const double *Xl = w.X + (size_t)b * w.sX + (size_t)l * t.K * J;
+    const double *xl = d.xit + (size_t)item * d.sxit;
+    double bmj = 0.0, amj = 0.0, cmj = 0.0;
+    if (j < M) {
+        bmj = t.bm0[j] + xl2 * t.cc[j];
+        if (j == 0) bmj = t.bm0[0] + (((m & 1) ? -1.0 : 1.0) - 1.0) * t.ammin + xl2 * t.cc[0];
+        amj = t.am[j];
+        cmj = t.cm[j];
+    }
+    float vmax = 0.0f;
+    for (int k = ty; k < 128; k += 8) {
+        float v = 0.0f;
+        if (k < NZ && j < M) {
+            // 4 pi G rho with the boundary folds (pot/pot3.f:212-224)
+            double r = t.pig4 * Xl[(size_t)k * J + j];
+            if (k == NZ - 1) r = r - t.cnmax * Xl[(size_t)NZ * J + j];
+            if (j == M - 1) r = r - t.cmmax * Xl[(size_t)k * J + M];
+            if (!kFirst) {
+                const double *xr = xl + (size_t)k * J;
+                double ax = (t.bn[k] + bmj) * xr[j];
+                if (k > 0) ax += t.an[k] * xl[(size_t)(k - 1) * J + j];
+                if (k < NZ - 1) ax += t.cn[k] * xl[(size_t)(k + 1) * J + j];
+                if (j > 0) ax += amj * xr[j - 1];
+                if (j < M - 1) ax += cmj * xr[j + 1];
+                r = r - ax;
+            }
+            v = (float)r;
+        }
+        tile[tx][k] = v;
+        vmax = fmaxf(vmax, fabsf(v));
+    }
+    __syncthreads();
+    float *Ri = d.R + (size_t)item * d.sro;
+    for (int e = threadIdx.x; e < 32 * 128; e += 256) {
+        const int jj = e >> 7, k = e & 127;
+        Ri[(size_t)(j0 + jj) * 128 + k] = tile[jj][k];
+    }
+    vmax = warp_max(vmax);
+    if ((threadIdx.x & 31) == 0) red[ty] = vmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float mx = red[0];
+        for (int i = 1; i < 8; ++i) mx = fmaxf(mx, red[i]);
+        if (mx > 0.0f) atomicMax(d.rmax + (size_t)item * d.nt + j0 / kWideN, __float_as_uint(mx));
+    }
+}
+
+// out[item][j][row] = sum_k A(row, k) in[item][j][k] for one 256-column tile:
+// A is the plan's 2^12-scaled FP16 hi/lo image of U or V, the input tile is
+// scaled by a power of two from its maximum and split to FP16 hi/lo in
+// shared memory, three MMA passes accumulate in FP32 in tensor memory.
+__global__ void __launch_bounds__(256, 1) k_wide_gemm(const uint8_t *aimg, const float *in, float *out,
+                                                      const unsigned *tmax, WideDev d, int *err)
+{
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tile = blockIdx.x, item = blockIdx.y;
+    uint8_t *sA = sm, *sBh = sm + kAImg, *sBl = sBh + (size_t)kWideN * 256;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sBl + (size_t)kWideN * 256);   // [0] product, [1] A tile
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bars + 2);
+    int *flag = reinterpret_cast<int *>(slot + 1);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        *flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_expect_tx(&bars[1], kAImg);
+        bulk_g2s(sA, aimg, kAImg, &bars[1]);
+    }
+    const float s = pow2_scale(__uint_as_float(tmax[(size_t)item * d.nt + tile]));
+    const float *src = in + (size_t)item * d.sro + (size_t)tile * kWideN * 128;
+    for (int i = tid; i < kWideN * 128; i += 256) put_split(sBh, sBl, i >> 7, i & 127, kWideN, src[i] * s);
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    // the A tile: every thread waits (bounded); a phase counts only if all saw it
+    bool a_ok = mbar_wait(&bars[1], 0);
+    if (!a_ok) *flag = 1;
+    __syncthreads();
+    a_ok = *flag == 0;
+    const uint32_t idesc = (1u << 4) | ((uint32_t)(kWideN >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    if (a_ok && tid == 0) gemm_issue(tmem, sA, sBh, kWideN, idesc, &bars[0]);
+    bool d_ok = a_ok && mbar_wait(&bars[0], 0);
+    if (a_ok && !d_ok) *flag = 1;
+    __syncthreads();
+    d_ok = *flag == 0;
+    tc_fence_after();
+    float *dst = out + (size_t)item * d.sro + (size_t)tile * kWideN * 128;
+    const int q = warp & 3, row = 32 * q + lane;
+    if (d_ok) {
+        const float unscale = 1.0f / (kAScale * s);
+        for (int c0 = (warp >> 2) * 128; c0 < (warp >> 2) * 128 + 128; c0 += 32) {
+            float v[32];
+            tm_ld32(tmem + ((uint32_t)(32 * q) << 16) + c0, v);
+#pragma unroll
+            for (int u = 0; u < 32; ++u) dst[(size_t)(c0 + u) * 128 + row] = v[u] * unscale;
+        }
+    } else {
+        // drain (bounded) what is still in flight, then make the tile NaN so the
+        // failure reaches PHI, and raise the error word
+        if (!a_ok) mbar_wait(&bars[1], 0);
+        else mbar_wait(&bars[0], 0);
+        for (int c0 = (warp >> 2) * 128; c0 < (warp >> 2) * 128 + 128; ++c0) dst[(size_t)c0 * 128 + row] = __int_as_float(0x7fc00000);
+        if (tid == 0) atomicExch(err, 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
+}
+
+// (T_r(m) + lam_p) w = W_p for each p (thread) of one item (block), with the
+// sweep table's pivot reciprocals and multipliers: rows [0, h) top-down,
+// [h, M) bottom-up, meeting at rows h-1 and h -- k_mode_mixed's sweeps on
+// CUDA cores.  W comes from O, w goes to R (zero past M and for p >= NZ).
+__global__ void __launch_bounds__(128) k_wide_sweep(DevTables t, MixedDev x, WideDev d)
+{
+    extern __shared__ float s_tab[];   // AM, CM as FP32 (M each)
+    float *s_am = s_tab, *s_cm = s_tab + t.M;
+    __shared__ float red[4][kWideTiles];
+    const int item = blockIdx.x, l = item % t.L, p = threadIdx.x, M = t.M;
+    const int m = l <= t.N ? l : l - t.N;
+    const int NTs = x.ntile, h = 32 * ((M + 63) / 64);
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+        s_am[j] = (float)t.am[j];
+        s_cm[j] = (float)t.cm[j];
+    }
+    __syncthreads();
+    const float *W = d.O + (size_t)item * d.sro + p;
+    float *wo = d.R + (size_t)item * d.sro + p;
+    const float *piv = x.sw_piv + (size_t)m * NTs * 128 + p, *mul = x.sw_mul + (size_t)m * NTs * 128 + p;
+    float tmx[kWideTiles];
+#pragma unroll
+    for (int i = 0; i < kWideTiles; ++i) tmx[i] = 0.0f;
+    if (p < t.NZ) {
+        float yp = 0.0f;
+#pragma unroll 8
+        for (int j = 0; j < h; ++j) {
+            const float rr = piv[(size_t)j * 128], ar = s_am[j] * rr;
+            yp = fmaf(-ar, yp, W[(size_t)j * 128] * rr);
+            wo[(size_t)j * 128] = yp;
+        }
+        const float yt = yp;
+        yp = 0.0f;
+#pragma unroll 8
+        for (int j = M - 1; j >= h; --j) {
+            const float rr = piv[(size_t)j * 128], cr = s_cm[j] * rr;
+            yp = fmaf(-cr, yp, W[(size_t)j * 128] * rr);
+            wo[(size_t)j * 128] = yp;
+        }
+        const float yu = yp, et = mul[(size_t)(h - 1) * 128], fu = mul[(size_t)h * 128];
+        const float xt = (yt + (1.0f - et) * yu) / ((et + fu) - et * fu);
+        const float xu = yu + (1.0f - fu) * xt;
+        float xn = xt;
+        wo[(size_t)(h - 1) * 128] = xt;
+        tmx[(h - 1) / kWideN] = fmaxf(tmx[(h - 1) / kWideN], fabsf(xt));
+#pragma unroll 8
+        for (int j = h - 2; j >= 0; --j) {
+            xn = wo[(size_t)j * 128] + (1.0f - mul[(size_t)j * 128]) * xn;
+            wo[(size_t)j * 128] = xn;
+            tmx[j / kWideN] = fmaxf(tmx[j / kWideN], fabsf(xn));
+        }
+        float xp = xu;
+        wo[(size_t)h * 128] = xu;
+        tmx[h / kWideN] = fmaxf(tmx[h / kWideN], fabsf(xu));
+#pragma unroll 8
+        for (int j = h + 1; j < M; ++j) {
+            xp = wo[(size_t)j * 128] + (1.0f - mul[(size_t)j * 128]) * xp;
+            wo[(size_t)j * 128] = xp;
+            tmx[j / kWideN] = fmaxf(tmx[j / kWideN], fabsf(xp));
+        }
+        for (int j = M; j < d.Jt; ++j) wo[(size_t)j * 128] = 0.0f;
+    } else {
+        for (int j = 0; j < d.Jt; ++j) wo[(size_t)j * 128] = 0.0f;
+    }
+    for (int i = 0; i < d.nt; ++i) {
+        const float v = warp_max(tmx[i]);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < d.nt) {
+        const float v = fmaxf(fmaxf(red[0][threadIdx.x], red[1][threadIdx.x]), fmaxf(red[2][threadIdx.x], red[3][threadIdx.x]));
+        if (v > 0.0f) atomicMax(d.wmax + (size_t)item * d.nt + threadIdx.x, __float_as_uint(v));
+    }
+}
+
+// x += delta (FP64) for one item per block; the last solve writes X's
+// interior.  Per-item sums of delta^2 and x^2 go to the correction report.
+__global__ void __launch_bounds__(256) k_wide_update(DevTables t, Work w, MixedDev x, WideDev d, int it, int last)
+{
+    __shared__ float tile[128][33];
+    __shared__ double red[2][8];
+    const int item = blockIdx.x, b = item / t.L, l = item % t.L, M = t.M, NZ = t.NZ, J = t.J;
+    double *Xl = w.X + (size_t)b * w.sX + (size_t)l * t.K * J;
+    double *xl = d.xit + (size_t)item * d.sxit;
+    const float *O = d.O + (size_t)item * d.sro;
+    double sd = 0.0, sx = 0.0;
+    for (int j0 = 0; j0 < M; j0 += 32) {
+        for (int e = threadIdx.x; e < 32 * 128; e += 256) {
+            const int jj = e >> 7, k = e & 127;
+            tile[k][jj] = O[(size_t)(j0 + jj) * 128 + k];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 32 * NZ; e += 256) {
+            const int k = e >> 5, jj = e & 31, j = j0 + jj;
+            if (j < M) {
+                const double dl = (double)tile[k][jj];
+                const size_t o = (size_t)k * J + j;
+                const double xn = (it > 0 ? xl[o] : 0.0) + dl;
+                if (last) Xl[o] = xn;
+                else xl[o] = xn;
+                sd += dl * dl;
+                sx += xn * xn;
+            }
+        }
+        __syncthreads();
+    }
+    sd = warp_sum(sd);
+    sx = warp_sum(sx);
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = sd;
+        red[1][threadIdx.x >> 5] = sx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, c = 0.0;
+        for (int i = 0; i < 8; ++i) {
+            a += red[0][i];
+            c += red[1][i];
+        }
+        double *cr = x.corr + (size_t)item * 16;
+        cr[2 * it] = a;
+        cr[2 * it + 1] = c;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 static int round64(int v) { return (v + 63) / 64 * 64; }
 
+// Grids the single-kernel mode solve covers; the others take the wide
+// pipeline.
+static bool mixed_fused(const chy::HostPlan *hp) { return hp->J % 16 == 0 && round64(hp->J) <= kMaxN; }
+
 bool chy_mixed_supported(const chy::HostPlan *hp)
 {
-    return hp->NZ <= 127 && hp->J >= 64 && hp->J % 16 == 0 && round64(hp->J) <= kMaxN;
+    return hp->NZ <= 127 && hp->J >= 64 && (mixed_fused(hp) || hp->J <= kWideMaxJ);
 }
 
 // Radial sweep table: for every azimuthal index m = 0..N and vertical
@@ -1208,8 +1496,9 @@ std::vector<float> chy::mixed_sweep_table(const chy::HostPlan &hp)
     return t;
 }
 
-size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image)
+size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image, bool mixed)
 {
+    if (!mixed) return image->size();
     // [U hi | U lo | V hi | V lo]: K-major swizzled FP16 tiles of 2^12 * U(p,k)
     // (rows p, K index k) and 2^12 * V(k,p) (rows k, K index p)
     std::vector<uint8_t> img((size_t)2 * kAImg, 0);
@@ -1249,7 +1538,7 @@ size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image)
 std::vector<double> chy::mixed_operand_tiles(const chy::HostPlan &hp)
 {
     std::vector<char> image;
-    const size_t off = chy_mixed_pack_tables(&hp, &image);
+    const size_t off = chy_mixed_pack_tables(&hp, &image, true);
     std::vector<double> out((size_t)4 * kTiles * kTiles);
     for (int t = 0; t < 4; ++t) {
         const size_t base = off + (size_t)(t >> 1) * kAImg + (size_t)(t & 1) * kTiles * kTiles * 2;
@@ -1266,6 +1555,7 @@ std::vector<double> chy::mixed_operand_tiles(const chy::HostPlan &hp)
 void chy_mixed_bind_tables(chy_plan *p, char *dev_base)
 {
     if (!p->mx) p->mx = new MixedState();
+    if (p->precision != CHY_PREC_MIXED) return;   // no mixed tables packed
     p->mx->dev.aimg = reinterpret_cast<const uint8_t *>(dev_base);
     size_t lam_off = (((size_t)(dev_base - p->d_tables) + 2 * kAImg) + 255) & ~(size_t)255;
     p->mx->dev.lam = reinterpret_cast<const float *>(p->d_tables + lam_off);
@@ -1277,11 +1567,20 @@ void chy_mixed_bind_tables(chy_plan *p, char *dev_base)
 // Per-mode correction sums and the error word; the FP64 iterate of the
 // general path (two or more corrections) is allocated by
 // chy_mixed_ensure_iterate when such a count is set.
+static size_t al32(size_t n) { return (n + 31) & ~(size_t)31; }   // doubles, 256-byte pieces
+
 size_t chy_mixed_work_doubles(const chy_plan *p)
 {
     if (p->precision != CHY_PREC_MIXED) return 0;
     const chy::HostPlan &hp = p->hp;
-    return (size_t)hp.L * 16 * p->max_batch + 8;
+    size_t n = al32((size_t)hp.L * 16 * p->max_batch + 8);
+    if (!mixed_fused(&hp)) {
+        const size_t items = (size_t)hp.L * p->max_batch, Jt = (size_t)(hp.J + 255) / 256 * 256;
+        n += al32(items * hp.K * hp.J);                  // iterate
+        n += 2 * al32(items * Jt * 128 / 2);             // R, O (FP32)
+        n += 2 * al32(items * (Jt / 256) / 2 + 1);       // rmax, wmax
+    }
+    return n;
 }
 
 void chy_mixed_bind_work(chy_plan *p, double *base)
@@ -1295,6 +1594,25 @@ void chy_mixed_bind_work(chy_plan *p, double *base)
     d.corr = base;
     d.err = reinterpret_cast<int *>(d.corr + d.scorr * p->max_batch);
     d.ntile = round64(hp.J);
+    if (p->precision == CHY_PREC_MIXED && !mixed_fused(&hp)) {
+        WideDev &wd = p->mx->wide;
+        p->mx->is_wide = true;
+        const size_t items = (size_t)hp.L * p->max_batch;
+        wd.Jt = (hp.J + 255) / 256 * 256;
+        wd.nt = wd.Jt / 256;
+        double *q = base + al32((size_t)hp.L * 16 * p->max_batch + 8);
+        wd.xit = q;
+        wd.sxit = (size_t)hp.K * hp.J;
+        q += al32(items * hp.K * hp.J);
+        wd.sro = (size_t)wd.Jt * 128;
+        wd.R = reinterpret_cast<float *>(q);
+        q += al32(items * wd.sro / 2);
+        wd.O = reinterpret_cast<float *>(q);
+        q += al32(items * wd.sro / 2);
+        wd.rmax = reinterpret_cast<unsigned *>(q);
+        q += al32(items * wd.nt / 2 + 1);
+        wd.wmax = reinterpret_cast<unsigned *>(q);
+    }
     if (p->precision == CHY_PREC_MIXED) {
         cudaMallocHost(&p->mx->h_corr, sizeof(double) * d.scorr * p->max_batch);
         cudaMallocHost(&p->mx->h_err, sizeof(int));
@@ -1316,9 +1634,35 @@ void chy_mixed_bind_work(chy_plan *p, double *base)
     }
 }
 
+static int wide_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
+{
+    const MixedDev &x = p->mx->dev;
+    const WideDev &d = p->mx->wide;
+    const chy::DevTables &t = p->t;
+    const int nit = std::min(1 + p->refine, 8), items = nb * t.L;
+    const size_t gsm = (size_t)kAImg + (size_t)kWideN * 512 + 64;
+    if (ensure_smem((const void *)k_wide_gemm, gsm) != cudaSuccess) return CHY_ERR_CUDA;
+    for (int it = 0; it < nit; ++it) {
+        const size_t mb = (size_t)items * d.nt * sizeof(unsigned);
+        if (cudaMemsetAsync(d.rmax, 0, mb, s) != cudaSuccess || cudaMemsetAsync(d.wmax, 0, mb, s) != cudaSuccess)
+            return CHY_ERR_CUDA;
+        const dim3 rg(d.Jt / 32, items), gg(d.nt, items);
+        if (it == 0) k_wide_resid<true><<<rg, 256, 0, s>>>(t, p->w, d, nb);
+        else k_wide_resid<false><<<rg, 256, 0, s>>>(t, p->w, d, nb);
+        k_wide_gemm<<<gg, 256, gsm, s>>>(x.aimg, d.R, d.O, d.rmax, d, x.err);
+        k_wide_sweep<<<items, 128, 2 * t.M * sizeof(float), s>>>(t, x, d);
+        k_wide_gemm<<<gg, 256, gsm, s>>>(x.aimg + kAImg, d.R, d.O, d.wmax, d, x.err);
+        k_wide_update<<<items, 256, 0, s>>>(t, p->w, x, d, it, it == nit - 1 ? 1 : 0);
+        if (cudaGetLastError() != cudaSuccess) return CHY_ERR_CUDA;
+    }
+    *launches = 5 * nit;
+    return CHY_OK;
+}
+
 int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
 {
     *launches = 0;
+    if (p->mx->is_wide) return wide_solve(p, nb, s, launches);
     MixedDev d = p->mx->dev;
     d.probe_polls = p->mx->probe_polls;
     d.nit = 1 + p->refine;
@@ -1400,7 +1744,8 @@ size_t chy_mixed_iterate_bytes(const chy_plan *p) { return p->mx ? p->mx->xbuf_b
 
 int chy_mixed_ensure_iterate(chy_plan *p)
 {
-    if (p->precision != CHY_PREC_MIXED || !p->mx || p->mx->dev.xbuf) return CHY_OK;
+    // the wide pipeline keeps its own FP64 iterate for any number of corrections
+    if (p->precision != CHY_PREC_MIXED || !p->mx || p->mx->dev.xbuf || p->mx->is_wide) return CHY_OK;
     MixedDev &d = p->mx->dev;
     const size_t bytes = d.sxb * p->max_batch * sizeof(double);
     if (cudaMalloc(&d.xbuf, bytes) != cudaSuccess) {

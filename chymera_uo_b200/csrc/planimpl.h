@@ -99,7 +99,7 @@ int chy_internal_run_batch(chy_plan *p, const chy::BatchPtrs &bp, int nb, cudaSt
 // Mixed-precision mode solve (k_mixed.cu).
 bool chy_mixed_supported(const chy::HostPlan *hp);
 // Appends the mixed path's tables to the packed table image; returns offset.
-size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image);
+size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image, bool mixed);
 void chy_mixed_bind_tables(chy_plan *p, char *dev_base);
 // Extra work-space doubles the mixed path needs (all batch slots).
 size_t chy_mixed_work_doubles(const chy_plan *p);

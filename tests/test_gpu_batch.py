@@ -59,3 +59,17 @@ def test_uneven_batch_alone_in_the_mix_and_from_a_graph(chylib):
     torch.cuda.synchronize()
     for (rho, g), m, f in zip(dens, mix, ref):
         assert _rel(m, f, g.jmax, g.kmax) <= 1e-10
+
+    # one density of each size class against the oracle
+    import numpy as np
+    from oracle import oracle as O
+    seen = set()
+    for (rho, g), m in zip(dens, mix):
+        key = (g.jmax, g.kmax, g.lmax)
+        if key in seen:
+            continue
+        seen.add(key)
+        oref = np.array(O.Oracle(*key, nthreads=8).solve(rho))
+        got = m.cpu().numpy()
+        ws = (slice(0, g.jmax + 1), slice(0, g.kmax + 1))
+        assert np.linalg.norm((got[ws] - oref[ws]).ravel()) <= 1e-10 * np.linalg.norm(oref[ws].ravel()), key

@@ -2,7 +2,9 @@
 Poisson clock while earlier ones are on the GPU; each result must equal the
 same density solved alone through a plain plan (bitwise: the kernels reduce in
 a fixed order per solve), mixed-precision results stay within rel. L2 1e-10
-of the FP64 path, and requests of one grid share batches."""
+of the FP64 path and, for one request of each size class, of the oracle, and
+requests of one grid share batches.  The mix includes a 512 x 128 x 512
+request, which the mixed server solves on its wide pipeline."""
 import threading
 
 import numpy as np
@@ -12,7 +14,7 @@ from chymera_uo_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [(64, 32, 64), (128, 64, 128), (64, 32, 128), (256, 128, 256), (128, 32, 64)]
+SIZES = [(64, 32, 64), (128, 64, 128), (64, 32, 128), (256, 128, 256), (128, 32, 64), (512, 128, 512)]
 
 
 def _requests(n, seed=7):
@@ -20,6 +22,8 @@ def _requests(n, seed=7):
     out = []
     for i in range(n):
         J, K, L = SIZES[int(rng.integers(len(SIZES)))] if i >= 8 else SIZES[0]
+        if i == n - 1:
+            J, K, L = SIZES[-1]   # one request of the largest class, at the end of the stream
         rho = synth.disk_density(J, K, L, 10**6 + i, slope=float(rng.uniform(-2, -1)),
                                  h=float(rng.uniform(0.03, 0.1)), spiral=True, spectrum=True)
         out.append(((J, K, L), rho))
@@ -55,7 +59,8 @@ def test_served_results_equal_solves_alone(chylib):
     assert stats["completed"] == len(reqs) and stats["batches"] < len(reqs)
     assert all(x > 0 for x in lat)
 
-    plans, plans64 = {}, {}
+    from oracle import oracle as O
+    plans, plans64, checked = {}, {}, set()
     for ((J, K, L), rho), (_, f) in zip(reqs, phis):
         key = (J, K, L)
         if key not in plans:
@@ -67,3 +72,9 @@ def test_served_results_equal_solves_alone(chylib):
         ws = (slice(0, J + 1), slice(0, K + 1))
         assert np.linalg.norm((f[ws] - ref[ws]).ravel()) <= 1e-10 * np.linalg.norm(ref[ws].ravel())
         assert np.all(f[:, K + 1, :] == 3.0)
+        if key not in checked:   # one request per size class against the oracle
+            checked.add(key)
+            o = O.Oracle(J, K, L, nthreads=8)
+            oref = np.array(o.solve(rho))
+            assert np.linalg.norm((f[ws] - oref[ws]).ravel()) <= 1e-10 * np.linalg.norm(oref[ws].ravel()), key
+    assert (512, 128, 512) in checked
