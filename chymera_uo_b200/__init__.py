@@ -61,6 +61,11 @@ class ChyExternal(C.Structure):
                 ("indirect", C.c_int), ("jmin", C.c_int)]
 
 
+class ChyBinary(C.Structure):
+    """The BINARY build's companion (pot/ExternalPot.f:57-69)."""
+    _fields_ = [("mass_bin", C.c_double), ("a_bin", C.c_double)]
+
+
 class ChySourceArgs(C.Structure):
     """SOURCE's arguments (radhydro/source.f:45-81); device pointers."""
     _fields_ = [("jmax", C.c_int), ("kmax", C.c_int), ("jmin", C.c_int), ("delt", C.c_double),
@@ -151,6 +156,8 @@ def lib():
         L.chy_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
         L.chy_server_get_stats.restype = i
         L.chy_server_destroy.argtypes = [vp]
+        L.chy_plan_set_binary.argtypes = [vp, C.POINTER(ChyBinary)]
+        L.chy_plan_set_binary.restype = i
         L.chy_plan_set_external.argtypes = [vp, C.POINTER(ChyExternal)]
         L.chy_plan_set_external.restype = i
         L.chy_plan_star_potential.argtypes = [vp, vp, i, vp]
@@ -252,6 +259,16 @@ class Plan:
             return
         e = ChyExternal(mass_star, tmassacc, rpstar, phi_star, int(indirect), jmin)
         _check(lib().chy_plan_set_external(self._p, C.byref(e)))
+
+    def set_binary(self, mass_bin: float | None = 1.0, a_bin: float = 100.0):
+        """Adds the BINARY build's companion term (pot/ExternalPot.f:57-69) to
+        the external potential of later solves (MASSBIN = 1, ABIN = 100 in
+        headers/units.h:25); ``mass_bin=None`` removes it."""
+        if mass_bin is None:
+            _check(lib().chy_plan_set_binary(self._p, None))
+            return
+        b = ChyBinary(mass_bin, a_bin)
+        _check(lib().chy_plan_set_binary(self._p, C.byref(b)))
 
     def star_potential(self, out=None, stream=None):
         """STARPHI(JMAX+2, KMAX+2, LMAX) of the plan's external potential:

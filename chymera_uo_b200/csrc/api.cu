@@ -58,6 +58,22 @@ struct Packer {
 
 static int ensure_host_staging(chy_plan *p);
 
+// getBinaryPosition's circular orbit (radhydro/ExternalRoutines.f:91-105):
+// MUBIN = MASSBIN + MASS_STAR, OMEGABIN = SQRT(MUBIN/ABIN**3), RBIN = ABIN,
+// and RCOM = RBIN - RBIN*MASS_STAR/MUBIN (pot/ExternalPot.f:15).
+static int set_binary_orbit(chy_plan *p)
+{
+    StarDev &x = p->star;
+    if (!x.binary) return CHY_OK;
+    const double mu = x.mass_bin + x.mass_star, a = p->bin_a;
+    const double omega = std::sqrt((mu) / (a * a * a));
+    x.rbin = a;
+    x.omega2 = omega * omega;
+    x.rcom = x.rbin - x.rbin * x.mass_star / mu;
+    return CHY_OK;
+}
+
+
 // The plan's arrays live on the device that was current at chy_plan_create;
 // launching with another device current would hand them to the wrong GPU.
 static int check_device(const chy_plan *p)
@@ -181,7 +197,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
     Packer pk;
     size_t o_twf = pk.vec(hp.fwd.twc), o_twonf = pk.vec(hp.fwd.onc), o_permf = pk.vec(hp.fwd.perm), o_rtf = pk.vec(hp.fwd.rt);
     size_t o_twi = pk.vec(hp.inv.twc), o_twoni = pk.vec(hp.inv.onc), o_permi = pk.vec(hp.inv.perm), o_rti = pk.vec(hp.inv.rt);
-    size_t o_cosm = pk.vec(hp.cosm), o_sinm = pk.vec(hp.sinm), o_fb = pk.vec(hp.fbasis);
+    size_t o_cosm = pk.vec(hp.cosm), o_sinm = pk.vec(hp.sinm), o_fb = pk.vec(hp.fbasis), o_bcos = pk.vec(hp.bcos);
     size_t o_rhf = pk.vec(hp.rhf), o_zhf = pk.vec(hp.zhf), o_r = pk.vec(hp.r);
     size_t o_rs = pk.vec(hp.ring_sorted), o_sring = pk.vec(hp.sring), o_sub = pk.vec(hp.sub_start);
     size_t o_sterm = pk.vec(hp.sterm);
@@ -229,6 +245,7 @@ int chy_plan_create(const chy_grid *g, int precision, int max_batch, chy_plan **
         return fail(CHY_ERR_DIMS, "no device transform for this LMAX");
     }
     t.cosm = (const double *)(D + o_cosm); t.sinm = (const double *)(D + o_sinm);
+    t.bcos = (const double *)(D + o_bcos);
     t.fbasis = (const double *)(D + o_fb);
     t.rhf = (const double *)(D + o_rhf); t.zhf = (const double *)(D + o_zhf); t.r = (const double *)(D + o_r);
     t.ring_sorted = (const int *)(D + o_rs); t.sring = (const double *)(D + o_sring);
@@ -363,8 +380,29 @@ int chy_plan_set_external(chy_plan *p, const chy_external *e)
         x.zof3n = hp.g.zof3n;
         x.dtheta = hp.dtheta;
     }
+    // the BINARY companion, if set, stays with the plan
+    x.binary = p->star.binary;
+    x.mass_bin = p->star.mass_bin;
+    x.rbin = p->star.rbin;
+    x.omega2 = p->star.omega2;
+    x.rcom = p->star.rcom;
+    x.mass_star = e ? e->mass_star : p->star.mass_star;
     p->star = x;
-    return CHY_OK;
+    return e ? set_binary_orbit(p) : CHY_OK;
+}
+
+int chy_plan_set_binary(chy_plan *p, const chy_binary *b)
+{
+    if (!p) return fail(CHY_ERR_ARG, "null plan");
+    if (!b) {
+        p->star.binary = 0;
+        return CHY_OK;
+    }
+    if (!(b->a_bin > 0.0)) return fail(CHY_ERR_ARG, "binary separation must be positive");
+    p->star.binary = 1;
+    p->star.mass_bin = b->mass_bin;
+    p->bin_a = b->a_bin;
+    return set_binary_orbit(p);
 }
 
 int chy_plan_star_potential(chy_plan *p, double *starphi, int ptr_kind, void *stream)

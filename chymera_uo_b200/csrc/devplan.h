@@ -65,6 +65,7 @@ struct DevTables {
     double sf1, pig4, grav, F1, cmmax, ammin, cnmax;
     FftDev fwd, inv;
     const double *cosm, *sinm;      // [10][L]
+    const double *bcos;             // [L] COS((L-1/2) DTHETA - PI) (the BINARY companion's angle)
     const double *rhf, *zhf;        // RHF(J+2), ZHF(K+2)
     const double *r;                // R(J+2)
     const double *fbasis;           // [21][L] transforms of {1, cos m psi, sin m psi}
@@ -108,6 +109,9 @@ struct StarDev {
     double mass_star = 0.0;
     double ix = 0.0, iy = 0.0;   // RPSTAR cos PHI_STAR, RPSTAR sin PHI_STAR
     double rof3n = 0.0, zof3n = 0.0, dtheta = 0.0;
+    // the BINARY build's companion (pot/ExternalPot.f:12-16, 57-69)
+    int binary = 0;
+    double mass_bin = 0.0, rbin = 0.0, omega2 = 0.0, rcom = 0.0;
 };
 constexpr int kDiagStar = 4;     // DIAG slots of INDIRECTX, INDIRECTY
 constexpr int kDiagPart = 8;     // first DIAG slot of the per-L moments

@@ -624,6 +624,24 @@ __device__ __forceinline__ double star_phi(const DevTables &t, const StarDev &x,
     return __ddiv_rn(-x.mass, __dsqrt_rn(q));
 }
 
+// The BINARY build's companion term (pot/ExternalPot.f:57-69) added to v, the
+// cell's PHI after STARPHI: v - MASSBIN/RDIST - HALF*OMEGABIN**2*((X+RCOM)**2
+// + Y**2) with RDIST = SQRT(RBIN**2 + RHF**2 - 2 RBIN RHF COS(THETA-PI) +
+// ZHF**2), X = RHF COS(THETA), Y = RHF SIN(THETA), THETA = (L-1/2) DTHETA,
+// in the reference's order of operations.
+__device__ __forceinline__ double binary_add(const DevTables &t, const StarDev &x, double v, int j, int k, int l)
+{
+    const double r = t.rhf[j], z = t.zhf[k];
+    double q = __dadd_rn(__dmul_rn(x.rbin, x.rbin), __dmul_rn(r, r));
+    q = __dsub_rn(q, __dmul_rn(__dmul_rn(__dmul_rn(2.0, x.rbin), r), t.bcos[l]));
+    q = __dadd_rn(q, __dmul_rn(z, z));
+    const double rdist = __dsqrt_rn(q);
+    const double xp = __dadd_rn(__dmul_rn(r, t.cosm[l]), x.rcom), yp = __dmul_rn(r, t.sinm[l]);
+    const double e = __dadd_rn(__dmul_rn(xp, xp), __dmul_rn(yp, yp));
+    v = __dsub_rn(v, __ddiv_rn(x.mass_bin, rdist));
+    return __dsub_rn(v, __dmul_rn(__dmul_rn(0.5, x.omega2), e));
+}
+
 // Star position of solve b: fixed, or the solve's INDIRECT shift.
 __device__ __forceinline__ void star_pos(const StarDev &x, const Work &w, int b, double *ix, double *iy)
 {
@@ -726,7 +744,9 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
     double ix = 0.0, iy = 0.0;
     if (x.on) star_pos(x, w, b, &ix, &iy);
     auto out = [&](int jj, int kk, int l, double v) -> double {
-        return x.on ? __dadd_rn(v, star_phi(t, x, ix, iy, jj, kk, l)) : v;
+        if (!x.on) return v;
+        v = __dadd_rn(v, star_phi(t, x, ix, iy, jj, kk, l));
+        return x.binary ? binary_add(t, x, v, jj, kk, l) : v;
     };
     auto store = [&](int i) {
         const int c = i % T::TC, l = i / T::TC, j = j0 + c;
@@ -814,7 +834,8 @@ __global__ void __launch_bounds__(128) k_star_rim(DevTables t, BatchPtrs bp, Wor
         // j < J2: row K = KMAX+2; j == J2: the cell (JMAX+2, 1)
         const int jj = j < J2 ? j : t.J + 1, kk = j < J2 ? t.K + 1 : 0;
         const size_t at = (size_t)jj + (size_t)J2 * ((size_t)kk + (size_t)K2 * l);
-        phi[at] = __dadd_rn(phi[at], star_phi(t, x, ix, iy, jj, kk, l));
+        const double v = __dadd_rn(phi[at], star_phi(t, x, ix, iy, jj, kk, l));
+        phi[at] = x.binary ? binary_add(t, x, v, jj, kk, l) : v;
     }
 }
 

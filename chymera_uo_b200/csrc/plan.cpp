@@ -523,6 +523,10 @@ int build_host_plan(const chy_grid &g, HostPlan &hp, std::string &err)
             hp.sinm[(size_t)(m - 1) * L + (l - 1)] = std::sin((double)m * psi);
         }
     }
+    // COS(THETA - PI), THETA = (L - 1/2) DTHETA: the BINARY companion's
+    // angle (pot/ExternalPot.f:56-62)
+    hp.bcos.resize(L);
+    for (int l = 1; l <= L; l++) hp.bcos[l - 1] = std::cos(((double)l - 0.5) * hp.dtheta - g.pi);
 
     // transforms of the boundary potential's azimuthal basis: the boundary
     // columns POT3 transforms (pot/pot3.f:93-140) are combinations of these

@@ -60,6 +60,7 @@ struct HostPlan {
 
     FftSchedule fwd, inv;
     std::vector<double> cosm, sinm;          // [m-1][l]  (m = 1..10)
+    std::vector<double> bcos;                // [l] COS((L-1/2) DTHETA - PI)
     // POT3's forward transform (times SF1) of the 21 azimuthal basis columns
     // {1, cos m psi_l, sin m psi_l}, m = 1..10: [q][mode]
     std::vector<double> fbasis;

@@ -42,7 +42,8 @@ struct chy_plan {
     double *coef_host = nullptr;   // /COEFS/ host destination (chy_plan_set_coef_host)
     double *coef_dev = nullptr;    // device COEF buffer owned by the plan
     size_t coef_bytes = 0;
-    chy::StarDev star;             // ExternalPot (chy_plan_set_external)
+    chy::StarDev star;             // ExternalPot (chy_plan_set_external, chy_plan_set_binary)
+    double bin_a = 0.0;            // the BINARY companion's separation ABIN
     int last_slot = 0;             // batch slot of the latest solve launched
     bool profile = false;
     // One event set per profiled launch sequence, read back lazily (after

@@ -211,6 +211,22 @@ typedef struct chy_external {
  * later solves through chy_solve / chy_solve_batch / chy_solve_multi.
  * chy_solve_static and the server solve POT3 alone. */
 int chy_plan_set_external(chy_plan *p, const chy_external *ext);
+/* The BINARY build's companion (pot/ExternalPot.f:12-16, 57-69), added after
+ * STARPHI on every cell while the external potential is set:
+ *   PHI = PHI - MASSBIN/RDIST - OMEGABIN**2/2 ((X+RCOM)**2 + Y**2),
+ *   RDIST = SQRT(RBIN**2 + RHF(J)**2 - 2 RBIN RHF(J) COS(THETA-PI) + ZHF(K)**2),
+ *   X, Y = RHF(J) COS(THETA), RHF(J) SIN(THETA), THETA = (L-1/2) DTHETA,
+ * for getBinaryPosition's circular orbit (radhydro/ExternalRoutines.f:91-105):
+ * MUBIN = MASSBIN + MASS_STAR, OMEGABIN = SQRT(MUBIN/ABIN**3), RBIN = ABIN,
+ * RCOM = RBIN - RBIN*MASS_STAR/MUBIN.  The reference's parameters are
+ * MASSBIN = 1, ABIN = 100 (headers/units.h:25).  STARPHI itself does not
+ * include it, as in the reference. */
+typedef struct chy_binary {
+    double mass_bin;             /* MASSBIN                                      */
+    double a_bin;                /* ABIN (> 0)                                   */
+} chy_binary;
+/* Sets (b non-NULL) or clears (NULL) the companion of the plan's later solves. */
+int chy_plan_set_binary(chy_plan *p, const chy_binary *b);
 /* Writes STARPHI(JMAX+2, KMAX+2, LMAX) (/GAP/ STARPHI) for the plan's
  * external potential: with `indirect`, for the star position of the plan's
  * latest solve (the last one of its most recent solve call), as the

@@ -55,6 +55,7 @@ def lib():
         L.ora_blktri.argtypes = [vp, i, i, i, dp, dp, dp, i, i, dp, dp, dp, i, dp, ip, dp]
         L.ora_blktri_wsize.restype = i
         L.ora_external_pot.argtypes = [vp, d, d, d, d, i, i, dp, dp]
+        L.ora_external_pot_binary.argtypes = [vp, d, d, d, d, i, i, i, d, d, dp, dp]
         L.ora_source.argtypes = [i, i, i, i, i, i, d, d, d, d, dp, dp, dp, dp, dp, dp, dp, dp]
         L.ora_blktri_wsize.argtypes = [i, i]
         _lib = L
@@ -173,13 +174,15 @@ class Oracle:
         return {"tmass": out[0], "phichk": out[1], "klocat": int(out[2])}
 
     def external_pot(self, mass_star: float, tmassacc: float = 0.0, rpstar: float = 0.0,
-                     phi_star: float = 0.0, indirect: bool = False, jmin: int = 2):
+                     phi_star: float = 0.0, indirect: bool = False, jmin: int = 2,
+                     binary: bool = False, mass_bin: float = 1.0, a_bin: float = 100.0):
         """ExternalPot (pot/ExternalPot.f:1-80) on the context's PHI: adds
-        STARPHI in place.  Returns (STARPHI, (INDIRECTX, INDIRECTY))."""
+        STARPHI in place, and with `binary` the BINARY build's companion term.
+        Returns (STARPHI, (INDIRECTX, INDIRECTY))."""
         sp = np.zeros((self.J + 2, self.K + 2, self.L), order="F")
         ixy = np.zeros(2)
-        lib().ora_external_pot(self._c, mass_star, tmassacc, rpstar, phi_star, int(indirect), jmin,
-                               _dp(sp), _dp(ixy))
+        lib().ora_external_pot_binary(self._c, mass_star, tmassacc, rpstar, phi_star, int(indirect), jmin,
+                                      int(binary), mass_bin, a_bin, _dp(sp), _dp(ixy))
         return sp, (float(ixy[0]), float(ixy[1]))
 
     def solve(self, rho: np.ndarray, delr: float | None = None, delz: float | None = None,

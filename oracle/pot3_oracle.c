@@ -2109,8 +2109,15 @@ void ora_pot3(ora_ctx *c, int npoint, int iprint)
  * and divided by -MASS_STAR.  STARPHI over the whole grid (ExternalPot.f:42-54)
  * is added to PHI and, if starphi is not NULL, stored there.  ixy (if not
  * NULL) receives INDIRECTX, INDIRECTY. */
-void ora_external_pot(ora_ctx *c, double mass_star, double tmassacc, double rpstar, double phi_star,
-                      int indirect, int jmin, double *starphi, double *ixy)
+/* ExternalPot (pot/ExternalPot.f:1-80), with the BINARY build's companion
+ * term when binary != 0: getBinaryPosition's circular orbit
+ * (radhydro/ExternalRoutines.f:91-105: muBin = massBin + mass_star,
+ * omegaBin = sqrt(muBin/aBin**3), rBin = aBin), rcom (ExternalPot.f:15) and
+ * PHI = PHI - massBin/rdist - half*omegaBin**2*((x+rcom)**2+y**2) per cell
+ * (ExternalPot.f:57-69). */
+void ora_external_pot_binary(ora_ctx *c, double mass_star, double tmassacc, double rpstar, double phi_star,
+                             int indirect, int jmin, int binary, double mass_bin, double a_bin, double *starphi,
+                             double *ixy)
 {
     const int jmax = c->jmax, kmax = c->kmax, lmax = c->lmax;
     const double dtheta = c->dtheta, half = 0.5, two = 2.0;
@@ -2129,8 +2136,18 @@ void ora_external_pot(ora_ctx *c, double mass_star, double tmassacc, double rpst
         iy = -(iy + sy) / mass_star;
     }
     const double mass = mass_star + tmassacc;
+    double rbin = 0.0, omega2 = 0.0, rcom = 0.0;
+    if (binary) {
+        const double mu = mass_bin + mass_star;
+        const double omega = sqrt((mu) / (a_bin * a_bin * a_bin));
+        rbin = a_bin;
+        omega2 = omega * omega;
+        rcom = rbin - rbin * mass_star / mu;
+    }
     for (int l = 1; l <= lmax; l++) {
         const double cl = cos(((double)(l - 1) + half) * dtheta), sl = sin(((double)(l - 1) + half) * dtheta);
+        const double theta = ((double)l - half) * dtheta;
+        const double cb = cos(theta - c->pi), ct = cos(theta), st = sin(theta);
         for (int k = 1; k <= kmax + 2; k++)
             for (int j = 1; j <= jmax + 2; j++) {
                 const double rhf = c->rhf[j - 1], zhf = c->zhf[k - 1];
@@ -2139,9 +2156,20 @@ void ora_external_pot(ora_ctx *c, double mass_star, double tmassacc, double rpst
                 PHI_(c, j, k, l) = PHI_(c, j, k, l) + sp;
                 if (starphi)
                     starphi[((size_t)j - 1) + (size_t)(jmax + 2) * (((size_t)k - 1) + (size_t)(kmax + 2) * ((size_t)l - 1))] = sp;
+                if (binary) {
+                    const double rdist = sqrt(rbin * rbin + rhf * rhf - two * rbin * rhf * cb + zhf * zhf);
+                    const double x = rhf * ct, y = rhf * st;
+                    PHI_(c, j, k, l) = PHI_(c, j, k, l) - mass_bin / rdist - half * omega2 * ((x + rcom) * (x + rcom) + y * y);
+                }
             }
     }
     if (ixy) { ixy[0] = ix; ixy[1] = iy; }
+}
+
+void ora_external_pot(ora_ctx *c, double mass_star, double tmassacc, double rpstar, double phi_star,
+                      int indirect, int jmin, double *starphi, double *ixy)
+{
+    ora_external_pot_binary(c, mass_star, tmassacc, rpstar, phi_star, indirect, jmin, 0, 0.0, 0.0, starphi, ixy);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -70,6 +70,11 @@ double *ora_phac(ora_ctx *c);
  * J = JMIN..JMAX1 (ExternalPot.f:21-40).  ixy (if not NULL) gets INDIRECTX/Y. */
 void ora_external_pot(ora_ctx *c, double mass_star, double tmassacc, double rpstar, double phi_star,
                       int indirect, int jmin, double *starphi, double *ixy);
+/* The same with the BINARY build's companion term (binary != 0): massBin,
+ * aBin as in headers/units.h:25 (1 and 100 there). */
+void ora_external_pot_binary(ora_ctx *c, double mass_star, double tmassacc, double rpstar, double phi_star,
+                             int indirect, int jmin, int binary, double mass_bin, double a_bin, double *starphi,
+                             double *ixy);
 
 /* SOURCE's potential, pressure and rotation terms (radhydro/source.f:45-81,
  * BINARY = 0) for a hydro grid jmax x kmax x lmax: omega, p, s, t, a are

@@ -175,3 +175,33 @@ def test_argument_checks(chylib):
     assert e.value.status == 13   # CHY_ERR_NOT_SETUP: no external potential set
     with pytest.raises(chylib.ChyError):
         plan.set_external(1.0, indirect=True, jmin=0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_binary_companion_is_the_reference_expression(chylib, ora, precision):
+    """The BINARY build's companion (pot/ExternalPot.f:57-69, orbit of
+    radhydro/ExternalRoutines.f:91-105) with the reference's MASSBIN = 1,
+    ABIN = 100: PHI with star and companion equals the oracle's ExternalPot
+    (STARPHI, then the companion term, in the reference's order) applied to
+    the same solve's PHI without them, bit for bit in every cell, through
+    host and device pointers; STARPHI itself is unchanged."""
+    import torch
+    rho, phi0 = density(3), phi_start(5)
+    plan = chylib.Plan(chylib.grid(J, K, L), precision, 1)
+    v, _ = host_solve(chylib, plan, rho, phi0)
+    plan.set_external(**STAR)
+    sp0 = plan.star_potential()
+    plan.set_binary(1.0, 100.0)
+    e, _ = host_solve(chylib, plan, rho, phi0)
+    o = ora.Oracle(J, K, L, nthreads=8)
+    o.phi[...] = v
+    sp, _ = o.external_pot(**STAR, binary=True, mass_bin=1.0, a_bin=100.0)
+    assert np.array_equal(e, np.array(o.phi))
+    assert np.array_equal(plan.star_potential(), sp0) and np.array_equal(sp0, sp)
+    assert not np.array_equal(e, v + sp)          # the companion term is there
+    ed = plan.solve(chylib.to_cuda_fortran(rho), chylib.to_cuda_fortran(phi0))
+    torch.cuda.synchronize()
+    assert np.array_equal(ed.cpu().numpy(), e)
+    plan.set_binary(None)
+    f, _ = host_solve(chylib, plan, rho, phi0)
+    assert np.array_equal(f, v + sp)
