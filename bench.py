@@ -261,6 +261,9 @@ def batched_record(steps, warmup, precisions=("mixed", "fp64", "blktri")):
         outs = [chy.fortran_zeros_cuda(p.shape) for p in plans]
         chy.solve_multi(plans, rhos, outs)          # side streams and smem attributes before capture
         torch.cuda.synchronize()
+        # the launch schedule of this request set, picked by timing (kept in the plans)
+        tune = chy.autotune_multi(plans, rhos, outs, repeats=2 if prec == "blktri" else 3)
+        torch.cuda.synchronize()
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
             chy.solve_multi(plans, rhos, outs)
@@ -277,7 +280,7 @@ def batched_record(steps, warmup, precisions=("mixed", "fp64", "blktri")):
             torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / k
         res[prec] = {"ms": ms, "outs": outs, "clocks": clk.summary(), "sizes": len(cache),
-                     "value": n / (ms * 1e-3), "steps": k}
+                     "value": n / (ms * 1e-3), "steps": k, "tune": tune}
         del graph, cache, plans
     worst = {}
     base = "blktri" if "blktri" in res else "fp64"
@@ -291,12 +294,15 @@ def batched_record(steps, warmup, precisions=("mixed", "fp64", "blktri")):
         worst[f"rel_l2_{prec}_vs_{base}_max"] = w
     rec = {"metric": "pot3 solves/s, 64 uneven grids per CUDA-graph replay", "unit": UNIT,
            "value": res["mixed"]["value"] if "mixed" in res else None,
-           "per_precision": {p: {"value": r["value"], "ms_per_step": r["ms"], "steps": r["steps"]}
+           "per_precision": {p: {"value": r["value"], "ms_per_step": r["ms"], "steps": r["steps"],
+                                 "schedule": r["tune"]}
                              for p, r in res.items()},
            "config": {"workload": "batched: 64 seeded disks, JMAX {64,128,256} x KMAX {32,64,128} x "
                                   "LMAX {64,128,256}, slope U[-2,-1], H/r U[0.03,0.1]",
                       "distinct_grids": next(iter(res.values()))["sizes"], "solves_per_step": n,
-                      "launch": "one CUDA graph replay of chy_solve_multi per step (grids on side streams)",
+                      "launch": "one CUDA graph replay of chy_solve_multi per step (grids on side streams), "
+                                "schedule picked by chy_autotune_multi before capture (schedule.ms_default: "
+                                "the default schedule's time per call, outside the graph)",
                       "l2": "inputs larger than L2 (all 64 densities resident)"},
            "accuracy": worst, "clocks": res[precisions[0]]["clocks"]}
     for p in res:

@@ -73,6 +73,15 @@ class ChySourceArgs(C.Structure):
                 ("s", C.c_void_p), ("t", C.c_void_p), ("a", C.c_void_p)]
 
 
+class ChyTune(C.Structure):
+    _fields_ = [("streams", C.c_int), ("chunk", C.c_int), ("mode_ctas", C.c_int), ("blk_warps", C.c_int),
+                ("blk_ctas_per_sm", C.c_int), ("ms", C.c_double), ("ms_default", C.c_double),
+                ("candidates", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("hbm_budget", C.c_longlong), ("precision", C.c_int), ("max_batch", C.c_int),
                 ("arena_fraction", C.c_double)]
@@ -143,6 +152,12 @@ def lib():
         L.chy_dbg_umma.restype = i
         L.chy_solve_multi.argtypes = [i, dpp, dpp, dpp, vp]
         L.chy_solve_multi.restype = i
+        L.chy_autotune_multi.argtypes = [i, dpp, dpp, dpp, vp, i, C.POINTER(ChyTune)]
+        L.chy_autotune_multi.restype = i
+        L.chy_plan_set_schedule.argtypes = [vp, C.POINTER(ChyTune)]
+        L.chy_plan_set_schedule.restype = i
+        L.chy_plan_get_schedule.argtypes = [vp, C.POINTER(ChyTune)]
+        L.chy_plan_get_schedule.restype = i
         L.chy_solve_static.argtypes = [vp, vp, vp, vp]
         L.chy_solve_static.restype = i
         L.chy_plan_set_coef_host.argtypes = [vp, vp]
@@ -156,6 +171,8 @@ def lib():
         L.chy_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
         L.chy_server_get_stats.restype = i
         L.chy_server_destroy.argtypes = [vp]
+        L.chy_plan_report.argtypes = [vp, C.c_char_p, ll]
+        L.chy_plan_report.restype = ll
         L.chy_plan_set_binary.argtypes = [vp, C.POINTER(ChyBinary)]
         L.chy_plan_set_binary.restype = i
         L.chy_plan_set_external.argtypes = [vp, C.POINTER(ChyExternal)]
@@ -259,6 +276,31 @@ class Plan:
             return
         e = ChyExternal(mass_star, tmassacc, rpstar, phi_star, int(indirect), jmin)
         _check(lib().chy_plan_set_external(self._p, C.byref(e)))
+
+    def report(self) -> str:
+        """The IPRINT = 1 unit-3 text of the latest solve (chy_plan_report);
+        needs the COEF output set (set_coef)."""
+        n = lib().chy_plan_report(self._p, None, 0)
+        if n < 0:
+            _check(-n)
+        buf = C.create_string_buffer(n + 1)
+        lib().chy_plan_report(self._p, buf, n + 1)
+        return buf.value.decode()
+
+    def schedule(self) -> dict:
+        """The plan's launch schedule (chy_plan_get_schedule)."""
+        t = ChyTune()
+        _check(lib().chy_plan_get_schedule(self._p, C.byref(t)))
+        d = t.as_dict()
+        for k in ("ms", "ms_default", "candidates"):
+            d.pop(k)
+        return d
+
+    def set_schedule(self, streams: int = 0, chunk: int = 0, mode_ctas: int = 0, blk_warps: int = 8,
+                     blk_ctas_per_sm: int = 2):
+        """Sets the plan's launch schedule (chy_plan_set_schedule)."""
+        t = ChyTune(streams, chunk, mode_ctas, blk_warps, blk_ctas_per_sm, 0.0, 0.0, 0)
+        _check(lib().chy_plan_set_schedule(self._p, C.byref(t)))
 
     def set_binary(self, mass_bin: float | None = 1.0, a_bin: float = 100.0):
         """Adds the BINARY build's companion term (pot/ExternalPot.f:57-69) to
@@ -447,6 +489,24 @@ def solve_multi(plans, rhos, phis=None, stream=None):
     s = torch.cuda.current_stream() if stream is None else stream
     _check(lib().chy_solve_multi(n, pp, rp, fp, C.c_void_p(s.cuda_stream)))
     return phis
+
+
+def autotune_multi(plans, rhos, phis=None, stream=None, repeats: int = 3) -> dict:
+    """Picks the launch schedule of chy_solve_multi for this request set by
+    timing candidates (chy_autotune_multi) and keeps it in the plans.
+    Synchronises; call it before capturing a graph.  Returns the choice and
+    the timings (ms per call, chosen and default)."""
+    import torch
+    n = len(rhos)
+    if phis is None:
+        phis = [fortran_zeros_cuda(p.shape, device=r.device) for p, r in zip(plans, rhos)]
+    pp = (C.c_void_p * n)(*[p._p.value for p in plans])
+    rp = (C.c_void_p * n)(*[r.data_ptr() for r in rhos])
+    fp = (C.c_void_p * n)(*[f.data_ptr() for f in phis])
+    s = torch.cuda.current_stream() if stream is None else stream
+    t = ChyTune()
+    _check(lib().chy_autotune_multi(n, pp, rp, fp, C.c_void_p(s.cuda_stream), repeats, C.byref(t)))
+    return t.as_dict()
 
 
 def fortran_zeros_cuda(shape, device="cuda"):

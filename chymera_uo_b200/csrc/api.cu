@@ -556,7 +556,7 @@ static int run_batch(chy_plan *p, const BatchPtrs &bp, int nb, cudaStream_t s)
         CHY_CUDA(launch_solve_fp64(t, p->w, nb, p->num_sms, s));
         nl = 3;
     } else if (p->precision == CHY_PREC_FP64_BLKTRI) {
-        CHY_CUDA(launch_solve_blk(t, p->w, nb, p->num_sms, s, &nl));
+        CHY_CUDA(launch_solve_blk(t, p->w, nb, p->num_sms, p->blk_warps, p->blk_ctas_per_sm, s, &nl));
     } else {
         int st = chy_mixed_solve(p, nb, s, &nl);
         if (st != CHY_OK) return st;
@@ -784,7 +784,10 @@ extern "C" int chy_solve_multi(int n, chy_plan *const *plans, const double *cons
     StreamPool *sp = nullptr;
     int st = stream_pool(&sp);
     if (st != CHY_OK) return st;
-    const int S = (int)std::min(order.size(), (size_t)kMultiStreams);
+    int nstreams = kMultiStreams;   // grids in flight at once: the smallest any plan asks for
+    for (chy_plan *p : order)
+        if (p->streams > 0) nstreams = std::min(nstreams, p->streams);
+    const int S = (int)std::min(order.size(), (size_t)nstreams);
     CHY_CUDA(cudaEventRecord(sp->fork, s));
     for (int i = 0; i < S; i++) CHY_CUDA(cudaStreamWaitEvent(sp->streams[i], sp->fork, 0));
     for (size_t r = 0; r < rank.size(); r++) {
@@ -792,8 +795,9 @@ extern "C" int chy_solve_multi(int n, chy_plan *const *plans, const double *cons
         chy_plan *p = order[g];
         const std::vector<int> &idx = members[g];
         cudaStream_t gs = sp->streams[r % S];
+        const int per = std::min(p->chunk > 0 ? std::min(p->chunk, p->max_batch) : p->max_batch, kMaxBatchPtrs);
         for (size_t first = 0; first < idx.size();) {
-            const int nb = (int)std::min(idx.size() - first, (size_t)std::min(p->max_batch, kMaxBatchPtrs));
+            const int nb = (int)std::min(idx.size() - first, (size_t)per);
             BatchPtrs bp{};
             for (int i = 0; i < nb; i++) {
                 bp.rho[i] = rho[idx[first + i]];
@@ -807,6 +811,142 @@ extern "C" int chy_solve_multi(int n, chy_plan *const *plans, const double *cons
     for (int i = 0; i < S; i++) {
         CHY_CUDA(cudaEventRecord(sp->join[i], sp->streams[i]));
         CHY_CUDA(cudaStreamWaitEvent(s, sp->join[i], 0));
+    }
+    return CHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// chy_autotune_multi: the launch schedule of a request set, picked by timing
+// ---------------------------------------------------------------------------
+namespace {
+struct Schedule {
+    int streams, chunk, mode_div, blk_warps, blk_cps;
+};
+
+void apply_schedule(const std::vector<chy_plan *> &plans, const Schedule &c)
+{
+    for (chy_plan *p : plans) {
+        p->streams = c.streams;
+        p->chunk = c.chunk;
+        p->mode_ctas = std::max(1, p->num_sms / c.mode_div);
+        p->blk_warps = c.blk_warps;
+        p->blk_ctas_per_sm = c.blk_cps;
+    }
+}
+}  // namespace
+
+extern "C" int chy_plan_set_schedule(chy_plan *p, const chy_tune *c)
+{
+    if (!p || !c) return fail(CHY_ERR_ARG, "null plan or schedule");
+    if (c->streams < 0 || c->streams > kMultiStreams || c->chunk < 0 || c->mode_ctas < 0 ||
+        !blk_schedule_valid(c->blk_warps, c->blk_ctas_per_sm))
+        return fail(CHY_ERR_ARG, "schedule out of range (streams 0..8, blk_warps 4/8/16, blk_warps * "
+                                 "blk_ctas_per_sm <= 16)");
+    p->streams = c->streams;
+    p->chunk = c->chunk;
+    p->mode_ctas = c->mode_ctas;
+    p->blk_warps = c->blk_warps;
+    p->blk_ctas_per_sm = c->blk_ctas_per_sm;
+    return CHY_OK;
+}
+
+extern "C" int chy_plan_get_schedule(const chy_plan *p, chy_tune *c)
+{
+    if (!p || !c) return fail(CHY_ERR_ARG, "null plan or schedule");
+    std::memset(c, 0, sizeof *c);
+    c->streams = p->streams;
+    c->chunk = p->chunk;
+    c->mode_ctas = p->mode_ctas;
+    c->blk_warps = p->blk_warps;
+    c->blk_ctas_per_sm = p->blk_ctas_per_sm;
+    return CHY_OK;
+}
+
+extern "C" int chy_autotune_multi(int n, chy_plan *const *plans, const double *const *rho, double *const *phi,
+                                  void *stream, int repeats, chy_tune *out)
+{
+    if (n <= 0 || !plans || !rho || !phi) return fail(CHY_ERR_ARG, "empty or null request set");
+    if (repeats < 1) repeats = 3;
+    std::vector<chy_plan *> uniq;
+    bool any_mixed = false, any_blk = false;
+    int max_batch = 1;
+    for (int i = 0; i < n; i++) {
+        if (!plans[i]) return fail(CHY_ERR_ARG, "null plan in request set");
+        if (std::find(uniq.begin(), uniq.end(), plans[i]) == uniq.end()) uniq.push_back(plans[i]);
+        any_mixed |= plans[i]->precision == CHY_PREC_MIXED;
+        any_blk |= plans[i]->precision == CHY_PREC_FP64_BLKTRI;
+        max_batch = std::max(max_batch, plans[i]->max_batch);
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CHY_CUDA(cudaEventCreate(&e0));
+    CHY_CUDA(cudaEventCreate(&e1));
+    auto measure = [&](const Schedule &c, double *ms) -> int {
+        apply_schedule(uniq, c);
+        int st = chy_solve_multi(n, plans, rho, phi, stream);   // warm-up
+        for (int r = 0; r < repeats && st == CHY_OK; r++) {
+            if (r == 0 && cudaEventRecord(e0, s) != cudaSuccess) return cuda_fail(cudaGetLastError(), "event");
+            st = chy_solve_multi(n, plans, rho, phi, stream);
+        }
+        if (st != CHY_OK) return st;
+        CHY_CUDA(cudaEventRecord(e1, s));
+        CHY_CUDA(cudaEventSynchronize(e1));
+        float f = 0.f;
+        CHY_CUDA(cudaEventElapsedTime(&f, e0, e1));
+        *ms = (double)f / repeats;
+        return CHY_OK;
+    };
+    // coordinate descent from the default schedule over each knob's values
+    Schedule best{kMultiStreams, 0, 1, 8, 2};
+    double best_ms = 0.0, default_ms = 0.0;
+    int st = measure(best, &best_ms), tried = 1;
+    default_ms = best_ms;
+    auto try_values = [&](auto set, const std::vector<int> &values) {
+        for (int v : values) {
+            if (st != CHY_OK) return;
+            Schedule c = best;
+            set(c, v);
+            if (std::memcmp(&c, &best, sizeof c) == 0) continue;
+            double ms = 0.0;
+            st = measure(c, &ms);
+            tried++;
+            if (st == CHY_OK && ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+    };
+    if (uniq.size() > 1) try_values([](Schedule &c, int v) { c.streams = v; }, {4, 2, 1});
+    if (max_batch > 1) try_values([](Schedule &c, int v) { c.chunk = v; }, {(max_batch + 1) / 2, (max_batch + 3) / 4});
+    if (any_mixed) try_values([](Schedule &c, int v) { c.mode_div = v; }, {2, 4});
+    if (any_blk) {
+        for (const auto &wc : std::vector<std::pair<int, int>>{{16, 1}, {4, 4}, {8, 1}, {4, 2}}) {
+            if (st != CHY_OK) break;
+            Schedule c = best;
+            c.blk_warps = wc.first;
+            c.blk_cps = wc.second;
+            double ms = 0.0;
+            st = measure(c, &ms);
+            tried++;
+            if (st == CHY_OK && ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    apply_schedule(uniq, best);
+    if (st != CHY_OK) return st;
+    if (out) {
+        out->streams = best.streams;
+        out->chunk = best.chunk;
+        out->mode_ctas = std::max(1, uniq[0]->num_sms / best.mode_div);
+        out->blk_warps = best.blk_warps;
+        out->blk_ctas_per_sm = best.blk_cps;
+        out->ms = best_ms;
+        out->ms_default = default_ms;
+        out->candidates = tried;
     }
     return CHY_OK;
 }

@@ -217,13 +217,38 @@ int main(int argc, char **argv)
     chy_plan *plan = nullptr;
     int st = chy_plan_create(&g, precision, 1, &plan);
     chy_diag d{};
+    // POT3(8, IPRINT=1): /COEFS/ for the unit-3 report (pot/pot3.f:402-418)
+    std::vector<double> coef((size_t)(J + 2) * (K + 2) * (L / 2) * 2, 0.0);
+    if (st == CHY_OK) st = chy_plan_set_coef_host(plan, coef.data());
     if (st == CHY_OK) st = chy_solve(plan, rho.data(), phi.data(), &d, CHY_PTR_HOST, nullptr);
+    std::string report;
+    if (st == CHY_OK) {
+        const long long n = chy_plan_report(plan, nullptr, 0);
+        if (n < 0) {
+            st = (int)-n;
+        } else {
+            report.resize((size_t)n + 1);
+            chy_plan_report(plan, &report[0], n + 1);
+            report.resize((size_t)n);
+        }
+    }
     if (st != CHY_OK) {
         std::fprintf(stderr, "chy_itype71: %s: %s\n", chy_status_string(st), chy_last_error());
         chy_plan_destroy(plan);
         return 1;
     }
     chy_plan_destroy(plan);
+    // unit 3 is not open yet in the reference's ITYPE=71 branch: gfortran's
+    // default connection writes the report to fort.3
+    {
+        const std::string p3 = dir + "/fort.3";
+        std::FILE *f3 = std::fopen(p3.c_str(), "w");
+        if (!f3 || std::fwrite(report.data(), 1, report.size(), f3) != report.size()) {
+            if (f3) std::fclose(f3);
+            return die("cannot write " + p3, 1);
+        }
+        std::fclose(f3);
+    }
     std::printf("TMASS=%.17g PHICHK=%.17g KLOCAT=%d\n", d.tmass, d.phichk, d.klocat);
 
     // ---- phi3d.NNNNNN (io.f:221-226)

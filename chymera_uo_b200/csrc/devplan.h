@@ -145,7 +145,11 @@ cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStrea
 cudaError_t launch_bdy_synth(const DevTables &t, const Work &w, int nb, cudaStream_t s);
 cudaError_t launch_solve_fp64(const DevTables &t, const Work &w, int nb, int num_sms, cudaStream_t s);
 // BLKTRI-order FP64 mode solves (k_blktri.cu): gather, cyclic reduction, scatter.
-cudaError_t launch_solve_blk(const DevTables &t, const Work &w, int nb, int num_sms, cudaStream_t s, int *launches);
+// Stage schedule: nw warps per CTA (4, 8 or 16), up to ctas_per_sm CTAs per SM,
+// nw * ctas_per_sm <= 16.
+cudaError_t launch_solve_blk(const DevTables &t, const Work &w, int nb, int num_sms, int nw, int ctas_per_sm,
+                             cudaStream_t s, int *launches);
+bool blk_schedule_valid(int nw, int ctas_per_sm);
 // Its work-space sizes in doubles: BVEC for nb solves, BSCR for a plan of max_batch.
 size_t blk_vector_doubles(const DevTables &t, int nb);
 size_t blk_scratch_doubles(const DevTables &t, int max_batch, int num_sms);

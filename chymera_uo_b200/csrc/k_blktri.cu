@@ -229,19 +229,15 @@ __global__ void __launch_bounds__(NW * 32) k_blk_solve(DevTables t, Work w, int 
     }
 }
 
-constexpr int kBlkWarps = 8;
-
-static int blk_solve_ctas(int ngroups, int num_sms)
-{
-    const int cap = 2 * num_sms;
-    return ngroups < cap ? ngroups : cap;
-}
-
 static int blk_groups(const DevTables &t, int nb) { return (nb * t.L + kBlkLanes - 1) / kBlkLanes; }
 
+// Scratch holds two vectors per warp for any stage schedule the launch accepts:
+// NW warps per CTA and up to ctas_per_sm CTAs per SM with NW * ctas_per_sm <= 16
+// (at most 16 warps per SM, at most one CTA per group).
 size_t blk_scratch_doubles(const DevTables &t, int max_batch, int num_sms)
 {
-    return (size_t)blk_solve_ctas(blk_groups(t, max_batch), num_sms) * kBlkWarps * 2 * (size_t)t.M * kBlkLanes;
+    const int g = blk_groups(t, max_batch);
+    return (size_t)16 * (g < num_sms ? g : num_sms) * 2 * (size_t)t.M * kBlkLanes;
 }
 
 size_t blk_vector_doubles(const DevTables &t, int nb)
@@ -249,16 +245,36 @@ size_t blk_vector_doubles(const DevTables &t, int nb)
     return (size_t)blk_groups(t, nb) * t.blk.nvec * (size_t)t.M * kBlkLanes;
 }
 
-cudaError_t launch_solve_blk(const DevTables &t, const Work &w, int nb, int num_sms, cudaStream_t s, int *launches)
+bool blk_schedule_valid(int nw, int ctas_per_sm)
 {
-    const int ngroups = blk_groups(t, nb);
+    return (nw == 4 || nw == 8 || nw == 16) && ctas_per_sm >= 1 && nw * ctas_per_sm <= 16;
+}
+
+template <int NW>
+static cudaError_t blk_launch(const DevTables &t, const Work &w, int ngroups, int ctas, cudaStream_t s)
+{
     const size_t smem = (size_t)2 * t.M * sizeof(double);
-    cudaError_t e = ensure_smem((const void *)k_blk_solve<kBlkWarps>, smem);
+    cudaError_t e = ensure_smem((const void *)k_blk_solve<NW>, smem);
     if (e != cudaSuccess) return e;
+    k_blk_solve<NW><<<ctas, NW * 32, smem, s>>>(t, w, ngroups);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_solve_blk(const DevTables &t, const Work &w, int nb, int num_sms, int nw, int ctas_per_sm,
+                             cudaStream_t s, int *launches)
+{
+    if (!blk_schedule_valid(nw, ctas_per_sm)) return cudaErrorInvalidValue;
+    const int ngroups = blk_groups(t, nb);
+    // one CTA per group at most; nw * ctas_per_sm <= 16 keeps the warps within
+    // the scratch (16 per SM, no more than 16 per group)
+    const int cap = ctas_per_sm * num_sms, ctas = ngroups < cap ? ngroups : cap;
     k_blk_gather<<<dim3(ngroups, t.NZ), 256, 0, s>>>(t, w, nb);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_blk_solve<kBlkWarps><<<blk_solve_ctas(ngroups, num_sms), kBlkWarps * 32, smem, s>>>(t, w, ngroups);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (nw == 4) e = blk_launch<4>(t, w, ngroups, ctas, s);
+    else if (nw == 8) e = blk_launch<8>(t, w, ngroups, ctas, s);
+    else e = blk_launch<16>(t, w, ngroups, ctas, s);
+    if (e != cudaSuccess) return e;
     k_blk_scatter<<<dim3(ngroups, t.NZ), 256, 0, s>>>(t, w, nb);
     if (launches) *launches = 3;
     return cudaGetLastError();

@@ -1678,7 +1678,8 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
     cudaError_t e = ensure_smem(kern, sm);
     if (e != cudaSuccess) return CHY_ERR_CUDA;
     const long long items = (long long)nb * p->hp.L;
-    const int grid = (int)(items < p->num_sms ? items : p->num_sms);
+    const int cap = p->mode_ctas > 0 && p->mode_ctas < p->num_sms ? p->mode_ctas : p->num_sms;
+    const int grid = (int)(items < cap ? items : cap);
     if (d.nit <= 2) k_mode_mixed<true><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x, p->mx->tm_xs);
     else k_mode_mixed<false><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x, p->mx->tm_xs);
     if (cudaGetLastError() != cudaSuccess) return CHY_ERR_CUDA;

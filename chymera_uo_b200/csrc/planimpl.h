@@ -22,6 +22,12 @@ struct chy_plan {
     int refine = 1;
     int num_sms = 148;
     int device = 0;                // the device the plan's tables and work space live on
+    // launch schedule (chy_autotune_multi picks these; 0 = the default)
+    int mode_ctas = 0;             // persistent CTAs of the fused mixed mode solve (default: one per SM)
+    int blk_warps = 8;             // BLKTRI order: warps per CTA (4, 8, 16)
+    int blk_ctas_per_sm = 2;       // BLKTRI order: CTAs per SM (blk_warps * this <= 16)
+    int chunk = 0;                 // chy_solve_multi: solves per launch sequence (default max_batch)
+    int streams = 0;               // chy_solve_multi: grids in flight at once (default 8)
     char *d_tables = nullptr;
     size_t table_bytes = 0;
     char *d_work = nullptr;

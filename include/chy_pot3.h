@@ -137,6 +137,35 @@ int chy_solve_batch(chy_plan *p, int n, const double *const *rho, double *const 
  * reference counterpart (the reference solves one grid per run). */
 int chy_solve_multi(int n, chy_plan *const *plans, const double *const *rho, double *const *phi, void *stream);
 
+/* Launch-schedule autotuner for a request set (no reference counterpart).
+ * Times chy_solve_multi over the given requests under candidate schedules
+ * and keeps the fastest in the plans, where later chy_solve_multi calls (and
+ * CUDA graphs captured after this call) use it:
+ *   streams      grids in flight at once (8, 4, 2, 1);
+ *   chunk        solves per launch sequence (max_batch, /2, /4);
+ *   mode_ctas    persistent CTAs of each fused mixed mode solve (all SMs, 1/2,
+ *                1/4: grids running side by side then share the SMs);
+ *   blk_warps,   the BLKTRI-order path's stage schedule: warps per CTA (the
+ *   blk_ctas_per_sm  cyclic-reduction tasks of a stage in flight at once) and
+ *                CTAs per SM.
+ * Search: from the default schedule, each knob in turn (coordinate descent),
+ * `repeats` timed calls per candidate after one warm-up call, CUDA events on
+ * `stream`.  The call synchronises `stream`; make it before any capture.  The
+ * results of the last call are in phi. */
+typedef struct chy_tune {
+    int streams, chunk, mode_ctas, blk_warps, blk_ctas_per_sm;
+    double ms;           /* one chy_solve_multi call under the chosen schedule */
+    double ms_default;   /* the same under the default schedule              */
+    int candidates;      /* schedules timed                                   */
+} chy_tune;
+int chy_autotune_multi(int n, chy_plan *const *plans, const double *const *rho, double *const *phi, void *stream,
+                       int repeats, chy_tune *out);
+/* A plan's launch schedule (the first five fields of chy_tune; 0 = default
+ * for streams, chunk and mode_ctas), e.g. to reuse a tuned schedule in a
+ * later run.  The timing fields are ignored / returned as 0. */
+int chy_plan_set_schedule(chy_plan *p, const chy_tune *c);
+int chy_plan_get_schedule(const chy_plan *p, chy_tune *c);
+
 /* ---- serving: continuous batching of solve requests ----------------------
  * No reference counterpart.  A server keeps one size class per distinct grid
  * (resident plans: tables + work space, two lanes so that the copies of one
@@ -181,6 +210,19 @@ int chy_plan_set_coef(chy_plan *p, double *coef_dev);
  * alone keep their values.  Host-pointer batches then run one solve per
  * chunk.  NULL stops the output. */
 int chy_plan_set_coef_host(chy_plan *p, double *coef_host);
+
+/* The text POT3 writes to unit 3 with IPRINT = 1 (pot/pot3.f:402-418), for
+ * the first solve of the plan's latest solve call: "PHAC(1:KMAX1):",
+ * PHAC(2:KMAX1) as FORMAT(1P11E11.3), "Fourier amplitudes and phases:" and,
+ * for LMAX > 8, per J = 2..JMAX the amplitudes and phases COEF(J,2,M,1:2),
+ * M = 1..8, as FORMAT(20X,I5,' COEFS=',1P8E12.3,/,25X,' PHASE=',0P8F12.2).
+ * Needs the COEF output of that solve (chy_plan_set_coef or
+ * chy_plan_set_coef_host; CHY_ERR_NOT_SETUP otherwise).  Synchronises the
+ * device.  Copies at most cap-1 characters and a NUL into buf and returns the
+ * full length, or a negative CHY_* status.  The ITYPE=71 run, which calls
+ * POT3 with IPRINT = 1 before unit 3 is opened (radhydro/io.f:208-218,
+ * :869), writes it to fort.3. */
+long long chy_plan_report(chy_plan *p, char *buf, long long cap);
 
 /* Fixed number of refinement corrections for CHY_PREC_MIXED, 0..7 (default
  * 1).  Up to one correction the first solution stays in tensor memory; two or

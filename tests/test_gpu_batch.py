@@ -73,3 +73,33 @@ def test_uneven_batch_alone_in_the_mix_and_from_a_graph(chylib):
         got = m.cpu().numpy()
         ws = (slice(0, g.jmax + 1), slice(0, g.kmax + 1))
         assert np.linalg.norm((got[ws] - oref[ws]).ravel()) <= 1e-10 * np.linalg.norm(oref[ws].ravel()), key
+
+
+@pytest.mark.parametrize("precision", ["mixed", "blktri"])
+def test_autotuned_schedule_keeps_results_bitwise(chylib, precision):
+    """chy_autotune_multi only changes how the work is launched (grids in
+    flight, solves per launch sequence, persistent CTAs, the BLKTRI stage
+    schedule), never what a solve computes: results after tuning, and from a
+    graph captured after it, equal the default schedule's bit for bit."""
+    import torch
+    dens = [synth.config_density(4, i) for i in range(8)]
+    rhos = [chylib.to_cuda_fortran(r) for r, _ in dens]
+    plans, cache = _plans(chylib, dens, precision, 4)
+    ref = chylib.solve_multi(plans, rhos)
+    torch.cuda.synchronize()
+    tune = chylib.autotune_multi(plans, rhos, repeats=2)
+    assert tune["candidates"] >= 3 and tune["ms"] <= tune["ms_default"]
+    assert tune["streams"] in (1, 2, 4, 8) and tune["blk_warps"] in (4, 8, 16)
+    assert tune["blk_warps"] * tune["blk_ctas_per_sm"] <= 16 and tune["mode_ctas"] >= 1
+    got = chylib.solve_multi(plans, rhos)
+    torch.cuda.synchronize()
+    for a, b in zip(got, ref):
+        assert torch.equal(a, b)
+    outs = [chylib.fortran_zeros_cuda(p.shape) for p in plans]
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        chylib.solve_multi(plans, rhos, outs)
+    graph.replay()
+    torch.cuda.synchronize()
+    for a, b in zip(outs, ref):
+        assert torch.equal(a, b)

@@ -128,3 +128,19 @@ def test_write_set_untouched_cells(chylib):
     phi = plan.solve(rho, np.full_like(rho, 7.0, order="F"))
     assert np.all(phi[:, K + 1, :] == 7.0) and np.all(phi[J + 1, 0, :] == 7.0)
     assert np.all(np.isfinite(phi))
+
+
+@pytest.mark.parametrize("nw,cps", [(4, 2), (4, 4), (8, 1), (16, 1)])
+def test_stage_schedules_give_the_same_modes(chylib, nw, cps):
+    """The stage schedule (warps per CTA, CTAs per SM) only changes which warp
+    runs which task: PHI is bitwise the default schedule's."""
+    import torch
+    J, K, L = 64, 32, 64
+    rho = chylib.to_cuda_fortran(synth.disk_density(J, K, L, 11, spiral=True, spectrum=True))
+    plan = chylib.Plan(chylib.grid(J, K, L), "blktri", 2)
+    ref = plan.solve_batch([rho, rho])
+    plan.set_schedule(blk_warps=nw, blk_ctas_per_sm=cps)
+    assert plan.schedule()["blk_warps"] == nw
+    got = plan.solve_batch([rho, rho])
+    torch.cuda.synchronize()
+    assert torch.equal(got[0], ref[0]) and torch.equal(got[1], ref[0])

@@ -277,3 +277,26 @@ def test_status_codes_on_device(chylib):
     assert L.chy_plan_create(C.byref(g), 0, 1, C.byref(p)) == 0
     assert L.chy_solve(p, None, None, None, 0, None) == 10
     L.chy_plan_destroy(p)
+
+
+@pytest.mark.parametrize("prec", ["blktri", "fp64"])
+def test_iprint_report_text(chylib, prec):
+    """chy_plan_report: the IPRINT = 1 unit-3 text (pot/pot3.f:402-418) of the
+    latest solve equals the reference's edit descriptors applied to the
+    oracle's PHAC and COEF, character for character."""
+    import sys, os
+    import torch
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from unit3 import report
+    from oracle import oracle as O
+    rho, g = synth.config_density(1)
+    J, K, L = 64, 32, 64
+    o = O.Oracle(J, K, L, nthreads=8, want_coef=True)
+    o.solve(rho)
+    plan = chylib.Plan(chylib.grid(J, K, L), prec, 1)
+    with pytest.raises(chylib.ChyError):
+        plan.report()                      # no COEF output set
+    coef = torch.zeros((2, L // 2, K + 2, J + 2), dtype=torch.float64, device="cuda").permute(3, 2, 1, 0)
+    plan.set_coef(coef)
+    plan.solve(chylib.to_cuda_fortran(rho))
+    assert plan.report() == report(lambda k: o.phac[k - 1], o.coef, J, K, L)

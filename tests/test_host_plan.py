@@ -212,3 +212,11 @@ def test_external_and_source_argument_checks(chylib):
     assert L.chy_source(None, None, None) == 10
     assert C.sizeof(chylib.ChyDiag) == 8 + 8 + 4 + 4 + 64 + 16
     assert C.sizeof(chylib.ChyExternal) == 4 * 8 + 2 * 4
+    assert C.sizeof(chylib.ChyBinary) == 2 * 8
+    b = chylib.ChyBinary(1.0, 100.0)
+    assert L.chy_plan_set_binary(None, C.byref(b)) == 10
+    assert C.sizeof(chylib.ChyTune) == 5 * 4 + 4 + 2 * 8 + 8
+    t = chylib.ChyTune()
+    assert L.chy_autotune_multi(0, None, None, None, None, 1, C.byref(t)) == 10
+    assert L.chy_plan_set_schedule(None, C.byref(t)) == 10
+    assert L.chy_plan_get_schedule(None, C.byref(t)) == 10
