@@ -575,7 +575,10 @@ def main():
     ap.add_argument("--batch", type=int, default=32, help="solves per step (launch sequence)")
     ap.add_argument("--impl", default="chymera", choices=["chymera", "reference"])
     ap.add_argument("--refine", type=int, default=1, help="mixed-precision refinement corrections")
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+    ap.add_argument("--grid", default=None,
+                    help="pot3 workload: JMAX,KMAX,LMAX of the timed solves (default 256,128,256; other "
+                         "grids are for profiling runs, not the metric)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "blktri"],
                     help="mode-solve path of the timed plan (fp64: the plain FP64 GPU path)")
     ap.add_argument("--latency-samples", type=int, default=200)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -593,6 +596,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.grid:
+        global J, K, L
+        J, K, L = (int(v) for v in args.grid.split(","))
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batch":
@@ -656,7 +662,9 @@ def main():
     hbm, peak_kind = peaks()
     achieved = alg / (mode_ms * 1e-3) / 1e9
     tps = profiled_traffic_per_solve() if args.precision == "mixed" else None
-    kname = "k_mode_mixed" if args.precision == "mixed" else "FP64 mode solves (k_zfwd_f64, k_thomas_f64, k_zinv_f64)"
+    kname = {"mixed": "k_mode_mixed" if J <= 256 else "wide mixed pipeline (k_wide_*)",
+             "fp64": "FP64 mode solves (k_zfwd_f64, k_thomas_f64, k_zinv_f64)",
+             "blktri": "BLKTRI-order mode solves (k_blk_gather, k_blk_solve, k_blk_scatter)"}[args.precision]
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
                 "traffic": None if tps is None else tps * B,

@@ -194,6 +194,7 @@ def test_binary_companion_is_the_reference_expression(chylib, ora, precision):
     plan.set_binary(1.0, 100.0)
     e, _ = host_solve(chylib, plan, rho, phi0)
     o = ora.Oracle(J, K, L, nthreads=8)
+    o.set_grid(1.0 / J, 0.5 / K)
     o.phi[...] = v
     sp, _ = o.external_pot(**STAR, binary=True, mass_bin=1.0, a_bin=100.0)
     assert np.array_equal(e, np.array(o.phi))
