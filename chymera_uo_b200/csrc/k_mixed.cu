@@ -1269,8 +1269,17 @@ __global__ void __launch_bounds__(256, 1) k_wide_gemm(const uint8_t *aimg, const
         bulk_g2s(sA, aimg, kAImg, &bars[1]);
     }
     const float s = pow2_scale(__uint_as_float(tmax[(size_t)item * d.nt + tile]));
-    const float *src = in + (size_t)item * d.sro + (size_t)tile * kWideN * 128;
-    for (int i = tid; i < kWideN * 128; i += 256) put_split(sBh, sBl, i >> 7, i & 127, kWideN, src[i] * s);
+    // the tile's rows as 16-byte loads, eight in flight per thread
+    const float4 *src = reinterpret_cast<const float4 *>(in + (size_t)item * d.sro + (size_t)tile * kWideN * 128);
+#pragma unroll 8
+    for (int i = tid; i < kWideN * 32; i += 256) {
+        const float4 v = src[i];
+        const int row = i >> 5, k = (i & 31) * 4;
+        put_split(sBh, sBl, row, k, kWideN, v.x * s);
+        put_split(sBh, sBl, row, k + 1, kWideN, v.y * s);
+        put_split(sBh, sBl, row, k + 2, kWideN, v.z * s);
+        put_split(sBh, sBl, row, k + 3, kWideN, v.w * s);
+    }
     fence_proxy_async();
     tc_fence_before();
     __syncthreads();

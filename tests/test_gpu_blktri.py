@@ -144,3 +144,24 @@ def test_stage_schedules_give_the_same_modes(chylib, nw, cps):
     got = plan.solve_batch([rho, rho])
     torch.cuda.synchronize()
     assert torch.equal(got[0], ref[0]) and torch.equal(got[1], ref[0])
+
+
+@functools.lru_cache(maxsize=None)
+def oracle_variant(isym, maxtrm, npoint, redge):
+    from oracle import oracle as O
+    rho, g = synth.config_density(1)
+    o = O.Oracle(64, 32, 64, nthreads=8)
+    phi = o.solve(rho, isym=isym, maxtrm=maxtrm, redge=redge, npoint=npoint)
+    return rho, phi
+
+
+@pytest.mark.parametrize("isym,maxtrm,npoint,redge", [(1, 10, 8, 0.0), (3, 8, 8, 0.0), (2, 4, 7, 0.0),
+                                                      (-2, 10, 8, 0.0), (2, 10, 8, 0.6)])
+def test_call_parameter_variants(chylib, isym, maxtrm, npoint, redge):
+    """ISYM, MAXTRM, NPOINT and REDGE as BDYGEN/ZAXPHI take them
+    (pot/boundary.f:97-105, pot/pot3.f:328-348), through the BLKTRI-order
+    mode solve: within 1e-12 of the oracle."""
+    rho, ref = oracle_variant(isym, maxtrm, npoint, redge)
+    phi, _, _ = solve(chylib, rho, 64, 32, 64, isym=isym, maxtrm=maxtrm, npoint=npoint, redge=redge)
+    ws = write_set(64, 32)
+    assert rel_l2(phi[ws], ref[ws]) < 1e-12

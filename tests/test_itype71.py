@@ -115,9 +115,10 @@ def test_phi3d_matches_the_oracle(chylib, tmp_path):
 def test_fort3_holds_the_iprint_report(chylib, tmp_path):
     """The ITYPE=71 branch calls POT3 with IPRINT = 1 before unit 3 is opened
     (radhydro/io.f:208-218, :869): the report goes to fort.3, text equal to
-    the reference's edit descriptors applied to the oracle's PHAC and COEF."""
+    the reference's edit descriptors applied to the oracle's PHAC and COEF
+    (PHAC's values within their printed precision)."""
     from oracle import oracle as O
-    from unit3 import report
+    from unit3 import check, report
     d = write_inputs(tmp_path)
     r = run(tmp_path)
     assert r.returncode == 0, r.stdout + r.stderr
@@ -125,5 +126,5 @@ def test_fort3_holds_the_iprint_report(chylib, tmp_path):
     o = O.Oracle(J, K, L, nthreads=4, want_coef=True)
     o.solve(expected_rho(d), delr=DELR, delz=DELZ)
     ref = report(lambda k: o.phac[k - 1], o.coef, J, K, L)
-    assert text == ref
+    check(text, ref)
     assert text.startswith("PHAC(1:KMAX1):\n") and text.count(" COEFS=") == J - 1

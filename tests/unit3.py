@@ -37,3 +37,22 @@ def report(phac_of_k, coef, J, K, L):
             out.append(" " * 20 + "%5d" % j + " COEFS=" + amp + "\n")
             out.append(" " * 25 + " PHASE=" + ph + "\n")
     return "".join(out)
+
+
+def check(text, ref, atol=1e-11):
+    """Every line of `text` equals the reference text character for
+    character, except the PHAC values, which are deviations 1 - PH/PHMAX of
+    order 1e-10 .. 1e-3: rounding noise of PHI moves them by about PHI's
+    relative error, so they are compared as numbers, within their printed
+    precision (half a unit in the 4th digit) plus atol."""
+    a, b = text.split("\n"), ref.split("\n")
+    assert len(a) == len(b), (len(a), len(b))
+    assert a[0] == b[0] == "PHAC(1:KMAX1):"
+    i = 1
+    while not b[i].startswith("Fourier"):
+        assert len(a[i]) == len(b[i])
+        for k in range(0, len(b[i]), 11):
+            x, y = float(a[i][k:k + 11]), float(b[i][k:k + 11])
+            assert abs(x - y) <= 5e-4 * abs(y) + atol, (i, k, a[i][k:k + 11], b[i][k:k + 11])
+        i += 1
+    assert a[i:] == b[i:]
