@@ -376,7 +376,8 @@ int chy_server_create(const chy_server_opts *o, chy_server **out)
     s->budget = (o && o->hbm_budget > 0) ? (size_t)o->hbm_budget : free_b / 4 * 3;
     s->precision = o ? o->precision : CHY_PREC_MIXED;
     s->max_batch = (o && o->max_batch > 0) ? std::min(o->max_batch, (int)kMaxBatchPtrs) : 8;
-    if (s->precision != CHY_PREC_FP64 && s->precision != CHY_PREC_MIXED) return CHY_ERR_ARG;
+    if (s->precision != CHY_PREC_FP64 && s->precision != CHY_PREC_MIXED && s->precision != CHY_PREC_FP64_BLKTRI)
+        return CHY_ERR_ARG;
     // request buffers get the arena fraction of the budget; plans the rest
     const double frac = (o && o->arena_fraction > 0.0 && o->arena_fraction < 1.0) ? o->arena_fraction : 0.5;
     const size_t arena = ((size_t)(s->budget * frac)) & ~(size_t)255;

@@ -178,7 +178,8 @@ int chy_plan_get_schedule(const chy_plan *p, chy_tune *c);
 typedef struct chy_server chy_server;
 typedef struct chy_server_opts {
     long long hbm_budget;      /* device bytes for plans + request buffers; 0: 3/4 of free */
-    int precision;             /* CHY_PREC_MIXED (grids it does not cover use FP64) or _FP64 */
+    int precision;             /* CHY_PREC_MIXED (grids it does not cover use FP64), _FP64 or */
+                               /* _FP64_BLKTRI                                                 */
     int max_batch;             /* solves per launch sequence (default 8, <= 64)            */
     double arena_fraction;     /* share of the budget for request buffers (default 0.5)    */
 } chy_server_opts;

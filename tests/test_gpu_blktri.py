@@ -68,7 +68,7 @@ def test_small_grid_meets_1e12(chylib, literal):
 
 
 @pytest.mark.parametrize("J,K,L", [(128, 64, 128), (64, 32, 256), (80, 32, 64), (65, 32, 64), (256, 64, 64),
-                                   (32, 8, 32)])
+                                   (32, 8, 32), (512, 128, 512)])
 def test_other_grid_sizes(chylib, J, K, L):
     rho, ref, _ = oracle_result((J, K, L), seed=31)
     phi, _, _ = solve(chylib, rho, J, K, L)

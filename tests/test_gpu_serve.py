@@ -78,3 +78,24 @@ def test_served_results_equal_solves_alone(chylib):
             oref = np.array(o.solve(rho))
             assert np.linalg.norm((f[ws] - oref[ws]).ravel()) <= 1e-10 * np.linalg.norm(oref[ws].ravel()), key
     assert (512, 128, 512) in checked
+
+
+def test_blktri_server_equals_plain_plan(chylib):
+    """A server of the BLKTRI-order path returns each request bitwise as a
+    plain plan of that path solves it."""
+    reqs = _requests(6, seed=3)
+    srv = chylib.Server("blktri", hbm_budget=16 << 30, max_batch=2)
+    bufs = []
+    for (J, K, L), rho in reqs[:5]:
+        a = chylib.pinned_fortran(rho.shape)
+        a[...] = rho
+        f = chylib.pinned_fortran(rho.shape)
+        f[...] = 0.0
+        bufs.append((a, f))
+    tickets = [srv.submit(chylib.grid(J, K, L), a, f) for ((J, K, L), _), (a, f) in zip(reqs[:5], bufs)]
+    for t in tickets:
+        srv.wait(t)
+    srv.close()
+    for ((J, K, L), rho), (_, f) in zip(reqs[:5], bufs):
+        alone = chylib.Plan(chylib.grid(J, K, L), "blktri", 1).solve(rho)
+        assert np.array_equal(alone, f), (J, K, L)
