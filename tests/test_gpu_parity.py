@@ -301,3 +301,55 @@ def test_iprint_report_text(chylib, prec):
     plan.set_coef(coef)
     plan.solve(chylib.to_cuda_fortran(rho))
     check(plan.report(), report(lambda k: o.phac[k - 1], o.coef, J, K, L))
+
+
+def test_fp64_paths_against_a_long_double_mode_solution(chylib, ora):
+    """At 256x128x256 the m = 0 mode system, with the device's right-hand side
+    (the oracle's forward transform, bitwise the device's, and the device's
+    boundary rows, folded in POT3's order), solved by sparse LU and refined
+    with long-double residuals: the FP64 eigenbasis path's mode is within
+    1e-12 of it (it is ~10x closer than BLKTRI's own rounding), and the
+    BLKTRI-order path's mode is within BLKTRI's 5e-12 floor."""
+    import ctypes as C
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    J, K, L = 256, 128, 256
+    M, NZ = J - 1, K - 1
+    rho, _ = synth.config_density(2)
+    g = chylib.grid(J, K, L)
+
+    def table(name, n):
+        out = np.zeros(n)
+        assert chylib.lib().chy_dbg_table(C.byref(g), name.encode(), out.ctypes.data_as(C.POINTER(C.c_double)), n) >= 0
+        return out
+
+    an, bn, cn = table("an", NZ), table("bn", NZ), table("cn", NZ)
+    am, cm = table("am", M), table("cm", M)
+    bm = table("blk_bm", L * M)[:M]                       # mode l = 0
+    sc = table("scalars", 8)
+    pig4, cmmax, cnmax = sc[1], sc[2], sc[4]
+    modes = {}
+    for prec in ("fp64", "blktri"):
+        plan = chylib.Plan(g, prec, 1)
+        plan.solve_batch([rho])
+        modes[prec] = plan.debug_work("X", L * K * J).reshape(L, K, J)[0]
+    X0 = modes["fp64"]
+    F0 = np.array([[ora.forward_real(rho[j + 1, k + 1, :].copy(), False)[0] for j in range(M)] for k in range(NZ)])
+    y = np.asfortranarray((pig4 * F0).T)
+    y[:, NZ - 1] = y[:, NZ - 1] - cnmax * X0[NZ, :M]
+    y[M - 1, :] = y[M - 1, :] - cmmax * X0[:NZ, M]
+    Tm = sp.diags([am[1:], bm, cm[:-1]], [-1, 0, 1])
+    Tn = sp.diags([an[1:], bn, cn[:-1]], [-1, 0, 1])
+    A = (sp.kron(Tn, sp.eye(M)) + sp.kron(sp.eye(NZ), Tm)).tocsc()
+    lu = spl.splu(A)
+    b = y.flatten(order="F")
+    x = lu.solve(b)
+    Al = A.astype(np.longdouble)
+    for _ in range(3):
+        r = b.astype(np.longdouble) - Al @ x.astype(np.longdouble)
+        x = x + lu.solve(r.astype(np.float64))
+    xt = x.reshape((M, NZ), order="F")
+    err = {p: float(np.linalg.norm(modes[p][:NZ, :M].T - xt) / np.linalg.norm(xt)) for p in modes}
+    assert err["fp64"] < 1e-12, err
+    assert err["blktri"] < 5e-12, err
+    assert err["fp64"] < err["blktri"], err
