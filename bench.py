@@ -662,7 +662,9 @@ def main():
     hbm, peak_kind = peaks()
     achieved = alg / (mode_ms * 1e-3) / 1e9
     tps = profiled_traffic_per_solve() if args.precision == "mixed" else None
-    kname = {"mixed": "k_mode_mixed" if J <= 256 else "wide mixed pipeline (k_wide_*)",
+    mixed_kernel = {1: "k_mode_mixed", 2: "k_mode_pair (CTA pairs, two modes per SM)",
+                    3: "wide mixed pipeline (k_wide_*)"}.get(chy.lib().chy_dbg_mixed_kernel(plan._p), "mixed")
+    kname = {"mixed": mixed_kernel,
              "fp64": "FP64 mode solves (k_zfwd_f64, k_thomas_f64, k_zinv_f64)",
              "blktri": "BLKTRI-order mode solves (k_blk_gather, k_blk_solve, k_blk_scatter)"}[args.precision]
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",

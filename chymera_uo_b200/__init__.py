@@ -75,8 +75,8 @@ class ChySourceArgs(C.Structure):
 
 class ChyTune(C.Structure):
     _fields_ = [("streams", C.c_int), ("chunk", C.c_int), ("mode_ctas", C.c_int), ("blk_warps", C.c_int),
-                ("blk_ctas_per_sm", C.c_int), ("ms", C.c_double), ("ms_default", C.c_double),
-                ("candidates", C.c_int)]
+                ("blk_ctas_per_sm", C.c_int), ("mode_kernel", C.c_int), ("ms", C.c_double),
+                ("ms_default", C.c_double), ("candidates", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -144,6 +144,8 @@ def lib():
         L.chy_dbg_table.restype = ll
         L.chy_dbg_mixed_probe.argtypes = [vp, i]
         L.chy_dbg_mixed_probe.restype = i
+        L.chy_dbg_mixed_kernel.argtypes = [vp]
+        L.chy_dbg_mixed_kernel.restype = i
         L.chy_dbg_blktri.argtypes = [C.POINTER(ChyGrid), i, C.POINTER(C.c_double)]
         L.chy_dbg_blktri.restype = i
         L.chy_dbg_work.argtypes = [vp, C.c_char_p, C.POINTER(C.c_double), ll]
@@ -297,9 +299,9 @@ class Plan:
         return d
 
     def set_schedule(self, streams: int = 0, chunk: int = 0, mode_ctas: int = 0, blk_warps: int = 8,
-                     blk_ctas_per_sm: int = 2):
+                     blk_ctas_per_sm: int = 2, mode_kernel: int = 0):
         """Sets the plan's launch schedule (chy_plan_set_schedule)."""
-        t = ChyTune(streams, chunk, mode_ctas, blk_warps, blk_ctas_per_sm, 0.0, 0.0, 0)
+        t = ChyTune(streams, chunk, mode_ctas, blk_warps, blk_ctas_per_sm, mode_kernel, 0.0, 0.0, 0)
         _check(lib().chy_plan_set_schedule(self._p, C.byref(t)))
 
     def set_binary(self, mass_bin: float | None = 1.0, a_bin: float = 100.0):

@@ -45,6 +45,9 @@ extern "C" long long chy_dbg_table(const chy_grid *g, const char *name, double *
     const std::string n(name);
     if (n == "U") return put(hp.U, out, cap);
     if (n == "V") return put(hp.V, out, cap);
+    if (n == "Qt") return put(hp.Qt, out, cap);
+    if (n == "dsc") return put(hp.dsc, out, cap);
+    if (n == "row_scales") return put(mixed_row_scales(hp), out, cap);
     if (n == "lam") return put(hp.lam, out, cap);
     if (n == "an") return put(hp.an, out, cap);
     if (n == "bn") return put(hp.bn, out, cap);

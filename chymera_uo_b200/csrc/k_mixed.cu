@@ -7,7 +7,11 @@
 // (see k_solve.cu) with
 //   * both vertical transforms on tcgen05 tensor cores: operands as FP16
 //     hi/lo pairs scaled by powers of two, three MMA passes (hi*hi + hi*lo +
-//     lo*hi) accumulated in FP32 in tensor memory -- about 22 bits;
+//     lo*hi) accumulated in FP32 in tensor memory -- about 22 bits.  The
+//     eigenbasis is used in its orthogonal form Q (U = Q^T D, V = D^-1 Q, D
+//     the diagonal symmetriser of the vertical operator), so one resident
+//     tile serves both transforms, read as Q^T and, through the transposed
+//     descriptor, as Q; D scales the residual rows and D^-1 the update;
 //   * the radial tridiagonal sweeps in FP32 on the accumulator rows, read and
 //     written in tensor memory, two threads per system (top-down and
 //     bottom-up elimination meeting in the middle).
@@ -15,8 +19,8 @@
 // refined solution converges to the FP64 solution of the same operator.
 //
 // One CTA owns one mode at a time (persistent over (solve, mode) items) and
-// keeps the mode's operand tiles in shared memory and its accumulators in
-// tensor memory; only Y, x, the eigenbasis tiles and the mode's slices of the
+// keeps the eigenbasis tile and the mode's operand tiles in shared memory and
+// its accumulators in tensor memory; only Y, x and the mode's slice of the
 // radial sweep table move through L2.
 // No TMA multicast is used anywhere.  Every wait is bounded: on a timeout the
 // kernel records an error word, stops issuing work, releases its tensor
@@ -73,8 +77,11 @@ __host__ __device__ inline uint32_t kmaj_off(int r, int k, int R)
 }  // namespace
 
 struct MixedDev {
-    const uint8_t *aimg;        // [U hi, U lo, V hi, V lo] swizzled tiles (2^12 scaled)
+    const uint8_t *aimg;        // [Q^T hi, Q^T lo] swizzled tile (2^12 scaled), Q the
+                                // orthogonal vertical eigenbasis
     const float *lam;           // [128]
+    const double *zsc;          // [4][128] per vertical row k: d_k, 1/d_k, d_k AN_k / d_(k-1),
+                                // d_k CN_k / d_(k+1) (D = diag(d) symmetrises T_z)
     const float *sw_mul;        // [N+1][ntile][128] multipliers e or f of the radial sweeps
     const float *sw_piv;        // [N+1][ntile][128] pivot reciprocals 1/D
     double *xbuf;               // [nb][L][K][J] FP64 iterate
@@ -110,6 +117,8 @@ struct MixedState {
     int probe_polls = 0;            // test hook (chy_dbg_mixed_probe)
     WideDev wide{};                 // the multi-kernel pipeline of grids k_mode_mixed does not cover
     bool is_wide = false;
+    int pair_clusters = -1;         // co-resident CTA pairs of k_mode_pair (-1: not asked yet)
+    bool paired = false;            // the last mode solve ran k_mode_pair (per-half sums)
     CUtensorMap tm_x{};             // X as rows of JMAX doubles: 16 x KMAX tiles, 128-byte swizzle
     CUtensorMap tm_xs{};            // the same with 16 x (KMAX-1) tiles: stores skip the boundary row
     bool tm_ok = false;
@@ -127,6 +136,16 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
     // start >> 4, LBO = 1 (unused for swizzled K-major), SBO = 1024 B >> 4,
     // version 1 (bit 46), layout SWIZZLE_128B (2 at bits 61-63)
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+// The same 128 x 128 tile read as an MN-major operand (its transpose): the
+// 64-element row chunks of the K-major layout are the 128-byte MN atoms.
+// LBO = 16 KB between the two 64-wide halves of M, SBO = 1 KB between groups
+// of eight K rows, SWIZZLE_128B.
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((kTiles * 128) >> 4) << 16) | (64ull << 32) |
+           (1ull << 46) | (2ull << 61);
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, int count)
@@ -398,22 +417,28 @@ __device__ __forceinline__ void split_rows32(uint8_t *hi, uint8_t *lo, const flo
 
 // Three-pass FP16 hi/lo product of the A tile (hi at sA, lo at sA + 32 KB)
 // and the B tile (hi at sBh, lo at sBh + NT*256) into TMEM columns [0, NT):
-// D = Ahi Bhi + Ahi Blo + Alo Bhi, K = 128 in eight 16-wide steps.  Issued by
-// one thread; completion is signalled on bar.
+// D = Ahi Bhi + Ahi Blo + Alo Bhi, K = 128 in eight 16-wide steps.  With
+// trans the A tile is used transposed (MN-major descriptor, the instruction's
+// transpose-A bit), so one resident tile serves both Q^T r and Q w.  Issued
+// by one thread; completion is signalled on bar.
 __device__ __forceinline__ void gemm_issue(uint32_t tmem, const uint8_t *sA, const uint8_t *sBh, int NT,
-                                           uint32_t idesc, uint64_t *bar)
+                                           uint32_t idesc, uint64_t *bar, bool trans)
 {
     tc_fence_after();
     const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sBh);
     const uint32_t a_lo = kTiles * kTiles * 2, b_lo = (uint32_t)NT * 256;
     const uint32_t pa[3] = {0u, 0u, a_lo}, pb[3] = {0u, b_lo, 0u};
+    const uint32_t id = idesc | (trans ? 1u << 15 : 0u);
 #pragma unroll
     for (int pass = 0; pass < 3; ++pass)
 #pragma unroll
         for (int kk = 0; kk < 8; ++kk) {
-            const uint32_t ao = a0 + pa[pass] + (uint32_t)(kk >> 2) * (kTiles * 128) + (uint32_t)(kk & 3) * 32;
+            // K-major: 16 K columns are 32 bytes of a 128-byte row, the second
+            // 64 in the next chunk; MN-major: 16 K rows are two 1 KB groups
+            const uint32_t ao = trans ? a0 + pa[pass] + (uint32_t)kk * 2048u
+                                      : a0 + pa[pass] + (uint32_t)(kk >> 2) * (kTiles * 128) + (uint32_t)(kk & 3) * 32;
             const uint32_t bo = b0 + pb[pass] + (uint32_t)(kk >> 2) * ((uint32_t)NT * 128) + (uint32_t)(kk & 3) * 32;
-            umma_f16(tmem, umma_desc(ao), umma_desc(bo), idesc, (pass | kk) ? 1u : 0u);
+            umma_f16(tmem, trans ? umma_desc_mn(ao) : umma_desc(ao), umma_desc(bo), id, (pass | kk) ? 1u : 0u);
         }
     umma_commit(bar);
 }
@@ -498,6 +523,14 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     const int kq = 32 * (warp & 3) + lane;     // TMEM lane this thread owns
     const int jh = warp >> 2;                  // which half of the columns
     const int NH = NT / 2;                     // columns per half (multiple of 8)
+    // Both transforms use the orthogonal Q (one resident tile, read as Q^T
+    // and as Q): W = U r = Q^T (D r) and delta = V w = D^-1 (Q w).  The
+    // residual is formed times d_k (this thread's row), the product Q w is
+    // scaled by 1/d_k; the stencil's vertical terms act on x0 without its 1/d
+    // factors, so their coefficients carry d_k/d_(k+-1).
+    const double dk = x.zsc[kq], ek = x.zsc[128 + kq];
+    const double an_s = x.zsc[256 + kq], cn_s = x.zsc[384 + kq];
+    const double pig4k = t.pig4 * dk, cnmaxk = t.cnmax * dk, cmmaxk = t.cmmax * dk;
     // MMA: kind::f16, A/B FP16 K-major, D FP32, M = 128, N = NT
     const uint32_t idesc = (1u << 4) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
     const int nit = kRes ? min(x.nit, 2) : x.nit;
@@ -519,7 +552,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     }
     if (tid == 0 && blockIdx.x < items && !failed) {
         mbar_expect_tx(bar_a, kAImg);
-        bulk_g2s(sA, x.aimg, kAImg, bar_a);   // U for the first transform
+        bulk_g2s(sA, x.aimg, kAImg, bar_a);   // Q, resident for every transform
     }
     bool a_inflight = blockIdx.x < items && !failed;
     long long fail_item = blockIdx.x;   // first item of this CTA left unsolved
@@ -647,7 +680,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 for (int c = 0; c < kRingSlots - 1; ++c) issue(c);
                 const int k = kq, jb = jh * 16, quad = warp & 3;
                 const bool krow = k < NZ;
-                const double an = d_an[k], cn = d_cn[k], bnk = d_bn[k];
+                const double an = an_s, cn = cn_s, bnk = d_bn[k];
                 for (int c = 0; c < nchr; ++c) {
                     const int c0 = c * kRingC;
                     float xc[16], xlf = 0.f, xrt = 0.f;
@@ -677,22 +710,23 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     if (*s_flag) break;   // a tile did not land: stop (uniform)
                     issue(c + kRingSlots - 1);
                     // right-hand side 4 pi G rho with the boundary folds
-                    // (pot/pot3.f:219-224): the row below the top boundary folds
-                    // row NZ (one thread), the column M fold lies in one chunk
+                    // (pot/pot3.f:219-224), times d_k: the row below the top
+                    // boundary folds row NZ (one thread), the column M fold
+                    // lies in one chunk
                     const uint8_t *slot = ring + (c % kRingSlots) * kRingSlot;
                     double yv[16];
 #pragma unroll
                     for (int u = 0; u < 16; u += 2) {
                         const double2 t2 = *reinterpret_cast<const double2 *>(at(slot, k, jb + u));
-                        yv[u] = t.pig4 * t2.x;
-                        yv[u + 1] = t.pig4 * t2.y;
+                        yv[u] = pig4k * t2.x;
+                        yv[u + 1] = pig4k * t2.y;
                     }
                     if (k == NZ - 1) {
 #pragma unroll
                         for (int u = 0; u < 16; u += 2) {
                             const double2 t3 = *reinterpret_cast<const double2 *>(at(slot, NZ, jb + u));
-                            yv[u] = fma(-t.cnmax, t3.x, yv[u]);
-                            yv[u + 1] = fma(-t.cnmax, t3.y, yv[u + 1]);
+                            yv[u] = fma(-cnmaxk, t3.x, yv[u]);
+                            yv[u + 1] = fma(-cnmaxk, t3.y, yv[u + 1]);
                         }
                     }
                     const int uM = M - 1 - (c0 + jb);   // uniform in the warp
@@ -701,7 +735,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                         ym_keep = yM;
 #pragma unroll
                         for (int u = 0; u < 16; ++u)
-                            if (u == uM) yv[u] = fma(-t.cmmax, yM, yv[u]);
+                            if (u == uM) yv[u] = fma(-cmmaxk, yM, yv[u]);
                     }
                     float v[16];
                     if (res_x) {
@@ -724,7 +758,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                             const float eu_u = eu[u] * zu, ed_u = ed[u] * zd;
                             xu = top0 ? eu_u : xu;
                             xd = bot31 ? ed_u : xd;
-                            // A x0 / u0: u0 is a power of two, so scaling the sum is exact
+                            // d_k A x0 / u0 (x0 = u0 t / d): u0 is a power of two, so
+                            // scaling the sum is exact
                             double ax = (bnk + d_bm[j]) * xd_[u + 1];
                             ax = fma(an, (double)xu, ax);
                             ax = fma(cn, (double)xd, ax);
@@ -827,7 +862,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                                 r = r - ax;
                             }
                         }
-                        v[u] = (float)r;
+                        v[u] = (float)(dk * r);
                         rmax = fmaxf(rmax, fabsf(v[u]));
                     }
                     tm_st8(tmem + lane_base + 256 + c0 + jb, v);
@@ -857,7 +892,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             // ---- W = U r (vertical transform) into TMEM cols [acc, acc + NT)
             if (a_inflight && !wait_all(bar_a, ph_a)) { failed = true; break; }
             a_inflight = false;
-            if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma);
+            if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma, false);
             mma_pend = true;
             // the first chunk of pivot reciprocals is loaded while the product runs
             const float *swp = x.sw_piv + (size_t)m * NT * 128 + kq;   // row j at swp[j * 128]
@@ -871,23 +906,21 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             tc_fence_after();
             float *cvs = reinterpret_cast<float *>(sBh);   // [j][p] multipliers for the back sweeps
             if (tid == 0) {
-                // B tile free: this m's multipliers for the back sweeps, then
-                // the A tile: V
+                // B tile free: this m's multipliers for the back sweeps
                 const float *src = x.sw_mul + (size_t)m * NT * 128;
                 mbar_expect_tx(bar_cv, (uint32_t)NT * 512);
                 for (int q = 0; q < 4; ++q) bulk_g2s(cvs + q * NT * 32, src + q * NT * 32, (uint32_t)NT * 128, bar_cv);
-                mbar_expect_tx(bar_a, kAImg);
-                bulk_g2s(sA, x.aimg + kAImg, kAImg, bar_a);
             }
             cv_pend = true;
-            a_inflight = true;
             // ---- radial sweeps (T_r(m) + lam_p) w = W_p, top-down over rows
             // [0, h) and bottom-up over [h, M), meeting in the middle.  The
             // multipliers and pivot reciprocals come from the sweep table, so
             // each row costs one dependent FMA.  The elimination reads the
             // pivot reciprocals from global memory one 32-row chunk ahead of
             // the recurrence; the multipliers, which only the back sweeps
-            // need, arrive in shared memory as one bulk copy meanwhile.
+            // need, arrive in shared memory as one bulk copy meanwhile.  The
+            // multipliers are in excess form (e_j, f_j small for small
+            // shifts), so 1 - e_j keeps nearly all of its bits.
             float xmax = 0.0f;
             {
                 const int p = kq;
@@ -1003,20 +1036,13 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             fence_proxy_async();
             tc_fence_before();
             __syncthreads();
-            // ---- delta = V w into TMEM cols [acc, acc + NT)
-            if (!wait_all(bar_a, ph_a)) { failed = true; break; }
-            a_inflight = false;
-            if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma);
+            // ---- Q w (delta times d) into TMEM cols [acc, acc + NT): the resident
+            // tile, transposed
+            if (tid == 0) gemm_issue(tmem + acc, sA, sBh, NT, idesc, bar_mma, true);
             mma_pend = true;
             if (!wait_all(bar_mma, ph_mma)) { failed = true; break; }
             mma_pend = false;
             tc_fence_after();
-            const bool more = !last || item + gridDim.x < items;
-            if (tid == 0 && more) {   // A tile free: U for the next transform
-                mbar_expect_tx(bar_a, kAImg);
-                bulk_g2s(sA, x.aimg, kAImg, bar_a);
-            }
-            a_inflight = more;
             const double unscale = 1.0 / ((double)kAScale * (double)kAScale * (double)s1 * (double)s2);
             if constexpr (kRes) {
                 if (!last) {
@@ -1031,6 +1057,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 // tensor-memory rows load while this chunk's tiles are stored.
                 double sd = 0.0, sx = 0.0;
                 const int jb = jh * 16, row0 = (b * t.L + l) * K;
+                const double uk = unscale * ek, u0k = u0 * ek;   // this row's 1/d_k
                 float dv[16], xv[16];
                 tm_ld16_nw(tmem + lane_base + acc + jb, dv);
                 if (res_x) tm_ld16_nw(tmem + lane_base + jb, xv);
@@ -1041,8 +1068,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
 #pragma unroll
                     for (int u = 0; u < 16; ++u) {
                         const int j = c0 + jb + u;
-                        const double dl = (double)dv[u] * unscale;
-                        xn[u] = (res_x ? (double)xv[u] * u0 : 0.0) + dl;
+                        const double dl = (double)dv[u] * uk;
+                        xn[u] = (res_x ? (double)xv[u] * u0k : 0.0) + dl;
                         if (kq < NZ && j < M) {
                             sd += dl * dl;
                             sx += xn[u] * xn[u];
@@ -1070,7 +1097,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 }
                 if (tid == 0) bulk_wait_all();   // tiles written, staging free for the next item
                 __syncthreads();
-                block_sum3(sd, sx, (double)sxf);
+                block_sum3(sd, sx, (double)sxf * ek * ek);
                 if (tid == 0) {
                     if (res_x) {   // the first solve's delta is x0 itself
                         cr[0] = d_red[16] * u0 * u0;
@@ -1112,7 +1139,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     float v[16];
                     tm_ld16(tmem + lane_base + c0 + jb, v);
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) sD[kq * 33 + jb + u] = (double)v[u] * unscale;
+                    for (int u = 0; u < 16; ++u) sD[kq * 33 + jb + u] = (double)v[u] * (unscale * ek);
                     __syncthreads();
                     const double *so = sO + (c & 1) * (128 * 32);
                     for (int i = tid; i < 128 * 32; i += 256) {
@@ -1168,6 +1195,665 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
 }
 
 // ---------------------------------------------------------------------------
+// The paired per-mode solver (two approximate solves, one correction)
+// ---------------------------------------------------------------------------
+// A cluster of two CTAs (two SMs) holds each (solve, mode) item: CTA r owns
+// the radial columns [r NH, (r + 1) NH), NH = ntile / 2 -- exactly the rows
+// that the two-sided radial elimination runs top-down (r = 0) and bottom-up
+// (r = 1), since h = 32 ceil(M / 64) = NH.  Half an item needs half of the
+// tensor memory (x0 and one accumulator of NH columns) and half of the
+// shared-memory operand region, so each CTA holds two items at once: its two
+// groups of four warps take different items and run independently, one
+// group's memory phases (right-hand-side intake, write-back) overlapping the
+// other's products and sweeps.  Per item, the two CTAs of a pair exchange
+// through distributed shared memory (st.async with complete-tx on the peer's
+// mbarrier, double-buffered) the rows where the radial sweeps meet, after
+// each elimination, and the iterate's edge column for the correction
+// residual.  Each CTA scales its half by its own powers of two; exchanged
+// values carry their exponents and are converted exactly.  The eigenbasis
+// tile is loaded once and shared by both groups.  Every wait is bounded.
+constexpr int kPairB = 64 * 1024;        // per-group region: ring, B tile, multipliers, staging
+constexpr int kPairTileB = 128 * 128;    // one 16-column x 128-row FP64 tile (bytes)
+constexpr int kPairRing = 4;             // residual ring slots (one tile each)
+constexpr int kPairStage = 4;            // write-back staging slots
+struct PairSmem {
+    static constexpr size_t a = 0;
+    static constexpr size_t b = kAImg;                              // [2][kPairB]
+    static constexpr size_t am = b + 2 * (size_t)kPairB;            // double [128] AM of this CTA's columns
+    static constexpr size_t cm = am + 128 * 8;                      // double [128] CM
+    static constexpr size_t bm = cm + 128 * 8;                      // double [2][128] BM_m per group
+    static constexpr size_t bn = bm + 2 * 128 * 8;                  // double [128] BN
+    static constexpr size_t ft = bn + 128 * 8;                      // float4 [128] {0, AM, CM, 0}
+    static constexpr size_t dred = ft + 128 * 16;                   // double [2][24]
+    static constexpr size_t fred = dred + 2 * 24 * 8;               // float [2][8]
+    static constexpr size_t edge = fred + 2 * 8 * 4;                // float [2][2][4][32]
+    static constexpr size_t xch = edge + 2 * 2 * 4 * 32 * 4;        // float4 [2][2][128] incoming exchanges
+    static constexpr size_t bars = xch + 2 * 2 * 128 * 16;          // uint64 [1 + 2 * 9]
+    static constexpr size_t misc = bars + 19 * 8;                   // tmem slot, flags [2]
+    static constexpr size_t bytes = misc + 16;
+};
+static_assert(PairSmem::bytes <= 227 * 1024, "pair shared memory");
+static_assert(PairSmem::xch % 16 == 0 && PairSmem::bars % 8 == 0, "pair alignment");
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_id_x()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_count_x()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+    return r;
+}
+// the peer CTA's shared::cluster address of a variable of this CTA
+__device__ __forceinline__ uint32_t peer_addr(const void *p, uint32_t peer)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(peer));
+    return r;
+}
+// 16 bytes into the peer's shared memory, counted on the peer's mbarrier
+__device__ __forceinline__ void st_async16(uint32_t raddr, float4 v, uint32_t rbar)
+{
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+                     raddr),
+                 "r"(__float_as_uint(v.x)), "r"(__float_as_uint(v.y)), "r"(__float_as_uint(v.z)),
+                 "r"(__float_as_uint(v.w)), "r"(rbar)
+                 : "memory");
+}
+// bounded wait with cluster-scope acquire (data written by the peer CTA)
+__device__ __forceinline__ bool mbar_wait_cl(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t a = smem_u32(bar);
+    for (long long i = 0; i < kSpinLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// power-of-two exponent k of pow2_scale(vmax) = 2^k
+__device__ __forceinline__ int pow2_exp(float vmax)
+{
+    if (!(vmax > 0.0f) || !isfinite(vmax)) return 0;
+    int e;
+    frexpf(vmax, &e);
+    return 14 - e;
+}
+
+__global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, MixedDev x, int nb,
+                                                      const __grid_constant__ CUtensorMap tm_x,
+                                                      const __grid_constant__ CUtensorMap tm_xs)
+{
+    extern __shared__ __align__(1024) uint8_t sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = warp >> 2, gt = tid & 127;            // group, thread in group
+    const uint32_t rank = cluster_rank(), peer = rank ^ 1u;
+    const int NT = x.ntile, NH = NT / 2, col0 = (int)rank * NH;
+    const int M = t.M, NZ = t.NZ, J = t.J, K = t.K;
+    uint8_t *sA = sm + PairSmem::a;
+    uint8_t *sB = sm + PairSmem::b + (size_t)g * kPairB;
+    uint8_t *sBh = sB, *sBl = sB + (size_t)NH * 256;
+    double *d_am = reinterpret_cast<double *>(sm + PairSmem::am);
+    double *d_cm = reinterpret_cast<double *>(sm + PairSmem::cm);
+    double *d_bm = reinterpret_cast<double *>(sm + PairSmem::bm) + g * 128;
+    double *d_bn = reinterpret_cast<double *>(sm + PairSmem::bn);
+    float4 *f_t = reinterpret_cast<float4 *>(sm + PairSmem::ft);
+    double *d_red = reinterpret_cast<double *>(sm + PairSmem::dred) + g * 24;
+    float *f_red = reinterpret_cast<float *>(sm + PairSmem::fred) + g * 8;
+    float *f_edge = reinterpret_cast<float *>(sm + PairSmem::edge) + g * 256;
+    float4 *xch = reinterpret_cast<float4 *>(sm + PairSmem::xch) + g * 256;   // [2 slots][128]
+    uint64_t *bar_a = reinterpret_cast<uint64_t *>(sm + PairSmem::bars);
+    uint64_t *gb = bar_a + 1 + g * 9;                   // this group's barriers
+    uint64_t *bar_mma = gb, *bar_ring = gb + 1, *bar_cv = gb + 5, *bar_x = gb + 6;   // bar_x[2]
+    uint64_t *bar_stagger = bar_a + 9;                  // group 0's gb[8]: group 1 may start
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + PairSmem::misc);
+    int *s_flag = reinterpret_cast<int *>(sm + PairSmem::misc + 8) ;   // [2]
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(bar_a, 1);
+        for (int i = 0; i < 18; ++i) mbar_init(bar_a + 1 + i, 1);
+        s_flag[0] = s_flag[1] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int jl = tid; jl < 128; jl += blockDim.x) {
+        const int j = col0 + jl;
+        const double a = (jl < NH && j < M) ? t.am[j] : 0.0, c = (jl < NH && j < M) ? t.cm[j] : 0.0;
+        d_am[jl] = a;
+        d_cm[jl] = c;
+        f_t[jl] = make_float4(0.f, (float)a, (float)c, 0.f);
+        d_bn[jl] = jl < NZ ? t.bn[jl] : 0.0;
+    }
+    tc_fence_before();
+    __syncthreads();
+    // the peer's barriers are initialised before anything is sent to them
+    cluster_sync_all();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+    const uint32_t G = (uint32_t)g * 256u;              // this group's tensor-memory columns
+    const int kq = 32 * (warp & 3) + lane;              // the row (TMEM lane) this thread owns
+    const double dk = x.zsc[kq], ek = x.zsc[128 + kq];
+    const double an_s = x.zsc[256 + kq], cn_s = x.zsc[384 + kq];
+    const double pig4k = t.pig4 * dk, cnmaxk = t.cnmax * dk, cmmaxk = t.cmmax * dk;
+    const uint32_t idesc = (1u << 4) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    const long long items = (long long)nb * t.L;
+    const long long pairs = cluster_count_x(), cl = cluster_id_x();
+    const long long first = 2 * cl + g, stride = 2 * pairs;
+    const int nch = NH / 16;
+    const int nit = x.nit < 2 ? 1 : 2;                 // approximate solves
+    const int h = NH;                                   // first bottom-up row (global)
+    const int clast = ((M - 1) / 32) * 32;              // the bottom-up sweep's first chunk (global)
+    // the peer's incoming-exchange slots and barriers for this group
+    const uint32_t r_xch = peer_addr(xch, peer), r_barx = peer_addr(bar_x, peer);
+
+    uint32_t ph_mma = 0, ph_cv = 0, ring_ph = 0, ring_pend = 0;
+    uint32_t xq = 0;                                    // exchanges so far (slot xq & 1)
+    bool mma_pend = false, cv_pend = false, failed = false;
+    bool a_wait = first < items;                        // this group still has to see Q land
+    long long fail_item = first;
+
+    if (x.probe_polls > 0) {
+        // test hook: a bounded wait on a barrier nothing arrives on, before
+        // anything is issued
+        if (tid == 0 && !mbar_wait_n(bar_a + 18, 0, x.probe_polls)) s_flag[0] = s_flag[1] = 1;
+        __syncthreads();
+        failed = s_flag[g] != 0;
+        a_wait = a_wait && !failed;
+    }
+    if (tid == 0 && 2 * cl < items && !failed) {
+        mbar_expect_tx(bar_a, kAImg);
+        bulk_g2s(sA, x.aimg, kAImg, bar_a);             // Q, shared by both groups for every transform
+    }
+    bool a_inflight = 2 * cl < items && !failed;        // drained by thread 0 at the end
+    // Group 1 starts when group 0 has finished its first item's last residual
+    // (about half an item): the two groups then stay out of step, one in its
+    // memory phases while the other runs its products and sweeps.  Group 0
+    // releases group 1 at the latest when it leaves its item loop.
+    bool stag_wait = g == 1 && first < items && !failed, stag_sent = g == 1;
+
+    auto gbar = [&]() { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); };
+    auto gwait = [&](uint64_t *bar, uint32_t &ph, bool cluster_scope) {
+        const bool ok = cluster_scope ? mbar_wait_cl(bar, ph) : mbar_wait(bar, ph);
+        if (!ok) s_flag[g] = 1;
+        gbar();
+        const bool good = s_flag[g] == 0;
+        if (good) ph ^= 1u;
+        return good;
+    };
+    // one DSMEM exchange with the peer: this thread's 16 bytes out, the
+    // peer's 16 bytes for the same row back (false on a timeout)
+    auto exchange = [&](float4 v, float4 &in) {
+        const uint32_t s = xq & 1u, par = (xq >> 1) & 1u;
+        st_async16(r_xch + (s * 128 + gt) * 16, v, r_barx + s * 8);
+        if (gt == 0) mbar_expect_tx(bar_x + s, 128 * 16);
+        uint32_t p = par;
+        const bool ok = gwait(bar_x + s, p, true);
+        ++xq;
+        if (ok) in = xch[s * 128 + gt];
+        return ok;
+    };
+    auto group_max = [&](float v) {
+        v = warp_max(v);
+        if (lane == 0) f_red[warp & 3] = v;
+        tc_fence_before();
+        gbar();
+        tc_fence_after();
+        return fmaxf(fmaxf(f_red[0], f_red[1]), fmaxf(f_red[2], f_red[3]));
+    };
+
+    for (long long item = first; item < items && !failed; item += stride) {
+        fail_item = item;
+        if (stag_wait) {
+            uint32_t ps = 0;
+            if (!gwait(bar_stagger, ps, false)) { failed = true; break; }
+            stag_wait = false;
+        }
+        const int o = (int)(item / nb), b = (int)(item % nb);
+        const int l = (o & 1) ? (o >> 1) + t.N : (o >> 1);
+        const int m = l <= t.N ? l : l - t.N;
+        const double xl2 = 2.0 * (t.xlamm[m] - 1.0);
+        {   // BM_m (pot/pot3.f:226-230) of this CTA's columns
+            const int jl = gt, j = col0 + jl;
+            double bm = 0.0;
+            if (jl < NH && j < M) {
+                bm = t.bm0[j] + xl2 * t.cc[j];
+                if (j == 0) bm = t.bm0[0] + (((m & 1) ? -1.0 : 1.0) - 1.0) * t.ammin + xl2 * t.cc[0];
+            }
+            d_bm[jl] = bm;
+        }
+        double *cr = x.corr + (size_t)b * x.scorr + (size_t)l * 16 + 8 * rank;
+        const int row0 = (b * t.L + l) * K;             // first tensor-map row of this item
+        double u0 = 0.0;                                // scale of x0 in tensor memory (2^eu0)
+        int eu0 = 0;
+        double ym_keep = 0.0, edge_in = 0.0;            // X(k, M); the peer's x0 edge in u0 units
+        float sxf = 0.f;
+        gbar();
+
+        for (int it = 0; it < nit && !failed; ++it) {
+            const bool res_x = it > 0;
+            const uint32_t acc = G + (res_x ? 128u : 0u);   // product / sweep columns
+            const uint32_t rcol = G + 128u;                 // residual columns
+            // ---- residual r = d_k (Y - A_m x) (FP64) -> TMEM as FP32, this
+            // CTA's columns in 16-column tiles through a four-slot ring
+            auto issue = [&](int c) {
+                if (c >= nch) return;
+                const int sl = c % kPairRing;
+                ring_pend |= 1u << sl;
+                if (warp != 4 * g) return;
+                uint8_t *slot = sB + sl * kPairTileB;
+                const int x0c = col0 + 16 * c;
+                if (x0c < J) {
+                    if (lane == 0) {
+                        mbar_expect_tx(bar_ring + sl, (uint32_t)(K * 128));
+                        tma_load_2d(slot, &tm_x, x0c, row0, bar_ring + sl);
+                    }
+                } else {
+                    for (int i = lane; i < K * 16; i += 32) reinterpret_cast<double *>(slot)[i] = 0.0;
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(bar_ring + sl);
+                }
+            };
+            auto landed = [&](int c) {
+                const int sl = c % kPairRing;
+                if (mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u)) {
+                    ring_ph ^= 1u << sl;
+                    ring_pend &= ~(1u << sl);
+                } else {
+                    s_flag[g] = 1;
+                }
+            };
+            auto at = [&](const uint8_t *slot, int k, int q) -> const double * {
+                return reinterpret_cast<const double *>(slot + k * 128 + ((((q >> 1) ^ (k & 7))) << 4) + ((q & 1) << 3));
+            };
+            fence_proxy_async();
+            gbar();
+            for (int c = 0; c < kPairRing - 1; ++c) issue(c);
+            const int k = kq, quad = warp & 3;
+            const bool krow = k < NZ;
+            const double bnk = d_bn[k];
+            float rmax = 0.0f;
+            for (int c = 0; c < nch; ++c) {
+                const int c0 = 16 * c;
+                float xc[16], xlf = 0.f, xrt = 0.f;
+                if (res_x) {
+                    const int jl = c0 - 1, jr = c0 + 16;
+                    tm_ld16_nw(tmem + lane_base + G + c0, xc);
+                    tm_ld1_nw(tmem + lane_base + G + (uint32_t)(jl < 0 ? 0 : jl), xlf);
+                    tm_ld1_nw(tmem + lane_base + G + (uint32_t)(jr < NH ? jr : NH - 1), xrt);
+                    landed(c);
+                    tm_wait_ld18(xc, xlf, xrt);
+                    float *ed = f_edge + ((c & 1) * 4 + quad) * 32;
+                    if (lane == 0) {
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) ed[u] = xc[u];
+                    }
+                    if (lane == 31) {
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) ed[16 + u] = xc[u];
+                    }
+                } else {
+                    landed(c);
+                }
+                gbar();
+                if (s_flag[g]) break;
+                issue(c + kPairRing - 1);
+                const uint8_t *slot = sB + (c % kPairRing) * kPairTileB;
+                double yv[16];
+#pragma unroll
+                for (int u = 0; u < 16; u += 2) {
+                    const double2 t2 = *reinterpret_cast<const double2 *>(at(slot, k, u));
+                    yv[u] = pig4k * t2.x;
+                    yv[u + 1] = pig4k * t2.y;
+                }
+                if (k == NZ - 1) {
+#pragma unroll
+                    for (int u = 0; u < 16; u += 2) {
+                        const double2 t3 = *reinterpret_cast<const double2 *>(at(slot, NZ, u));
+                        yv[u] = fma(-cnmaxk, t3.x, yv[u]);
+                        yv[u + 1] = fma(-cnmaxk, t3.y, yv[u + 1]);
+                    }
+                }
+                const int uM = M - 1 - (col0 + c0);     // column M lies in the tile of column M-1
+                if (uM >= 0 && uM < 16) {
+                    const double yM = *at(slot, k, uM + 1);
+                    ym_keep = yM;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                        if (u == uM) yv[u] = fma(-cmmaxk, yM, yv[u]);
+                }
+                float v[16];
+                if (res_x) {
+                    const float *eu = f_edge + ((c & 1) * 4 + (quad > 0 ? quad - 1 : quad)) * 32 + 16;
+                    const float *ed = f_edge + ((c & 1) * 4 + (quad < 3 ? quad + 1 : quad)) * 32;
+                    const bool top0 = lane == 0, bot31 = lane == 31;
+                    const float zu = quad > 0 ? 1.f : 0.f, zd = quad < 3 ? 1.f : 0.f;
+                    double xd_[18];
+                    // the neighbours across the pair's column boundary come from the peer
+                    xd_[0] = c0 == 0 ? (rank == 1 ? edge_in : 0.0) : (double)xlf;
+                    xd_[17] = c0 + 16 == NH ? (rank == 0 ? edge_in : 0.0) : (double)xrt;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) xd_[u + 1] = (double)xc[u];
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const int jl = c0 + u, j = col0 + jl;
+                        float xu = __shfl_up_sync(0xffffffffu, xc[u], 1);
+                        float xd = __shfl_down_sync(0xffffffffu, xc[u], 1);
+                        const float eu_u = eu[u] * zu, ed_u = ed[u] * zd;
+                        xu = top0 ? eu_u : xu;
+                        xd = bot31 ? ed_u : xd;
+                        double ax = (bnk + d_bm[jl]) * xd_[u + 1];
+                        ax = fma(an_s, (double)xu, ax);
+                        ax = fma(cn_s, (double)xd, ax);
+                        ax = fma(d_am[jl], xd_[u], ax);
+                        ax = fma(d_cm[jl], xd_[u + 2], ax);
+                        const double r = fma(-u0, ax, yv[u]);
+                        const bool in = krow && j < M;
+                        sxf = fmaf(in ? xc[u] : 0.f, xc[u], sxf);
+                        v[u] = in ? (float)r : 0.f;
+                        rmax = fmaxf(rmax, fabsf(v[u]));
+                    }
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) {
+                        const int j = col0 + c0 + u;
+                        v[u] = (krow && j < M) ? (float)yv[u] : 0.f;
+                        rmax = fmaxf(rmax, fabsf(v[u]));
+                    }
+                }
+                tm_st16_nw(tmem + lane_base + rcol + c0, v);
+            }
+            tm_wait_st();
+            if (s_flag[g]) { failed = true; break; }
+            if (!stag_sent && it == nit - 1) {
+                if (gt == 0) mbar_arrive(bar_stagger);
+                stag_sent = true;
+            }
+            const int k1 = pow2_exp(group_max(rmax));
+            const float s1 = ldexpf(1.0f, k1);
+            // ---- TMEM r -> B tile (row j, K index k), FP16 hi/lo
+            for (int c0 = 0; c0 < NH; c0 += 32) {
+                float v[32];
+                tm_ld32(tmem + lane_base + rcol + c0, v);
+#pragma unroll
+                for (int u = 0; u < 32; ++u) v[u] *= s1;
+                split_rows32(sBh, sBl, v, c0, kq, lane, NH);
+            }
+            fence_proxy_async();
+            tc_fence_before();
+            gbar();
+            // ---- W = Q^T r into TMEM cols [acc, acc + NH)
+            if (a_wait) {
+                uint32_t pa = 0;
+                if (!gwait(bar_a, pa, false)) { failed = true; break; }
+                a_wait = false;
+            }
+            if (gt == 0) gemm_issue(tmem + acc, sA, sBh, NH, idesc, bar_mma, false);
+            mma_pend = true;
+            // the first chunk of pivot reciprocals is loaded while the product runs
+            const float *swp = x.sw_piv + (size_t)m * NT * 128 + kq;    // global row j at swp[j * 128]
+            float R[32];
+#pragma unroll
+            for (int u = 0; u < 32; ++u) R[u] = swp[(size_t)((rank == 0 ? 0 : clast) + u) * 128];
+            if (!gwait(bar_mma, ph_mma, false)) { failed = true; break; }
+            mma_pend = false;
+            tc_fence_after();
+            float *cvs = reinterpret_cast<float *>(sB);   // [local row][p] multipliers
+            if (gt == 0) {
+                const float *src = x.sw_mul + ((size_t)m * NT + col0) * 128;
+                mbar_expect_tx(bar_cv, (uint32_t)NH * 512);
+                for (int q = 0; q < 4; ++q) bulk_g2s(cvs + q * NH * 32, src + q * NH * 32, (uint32_t)NH * 128, bar_cv);
+            }
+            cv_pend = true;
+            // ---- radial sweeps (T_r(m) + lam_p) w = W_p on this CTA's rows:
+            // top-down over [0, h) (rank 0) or bottom-up over [h, M) (rank 1),
+            // then the meeting rows h-1 and h from both, then the back sweep
+            float xmax = 0.0f;
+            const int p = kq;
+            const bool live = p < NZ;
+            const uint32_t tb = tmem + lane_base + acc;
+            const int ks = 12 + k1;                     // the sweep values are 2^ks times W
+            {
+                float yv[32], Rn[32];
+                float yp = 0.f;
+                if (rank == 0) {
+                    for (int c0 = 0; c0 < NH; c0 += 32) {
+                        if (c0 + 32 < NH) {
+#pragma unroll
+                            for (int u = 0; u < 32; ++u) Rn[u] = swp[(size_t)(c0 + 32 + u) * 128];
+                        }
+                        tm_ld32(tb + c0, yv);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) {
+                            const float rr = R[u], ar = f_t[c0 + u].y * rr;
+                            yp = fmaf(-ar, yp, yv[u] * rr);
+                            yv[u] = yp;
+                        }
+                        tm_st32_nw(tb + c0, yv);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) R[u] = Rn[u];
+                    }
+                } else {
+                    for (int c0 = clast; c0 >= h; c0 -= 32) {
+                        if (c0 - 32 >= h) {
+#pragma unroll
+                            for (int u = 0; u < 32; ++u) Rn[u] = swp[(size_t)(c0 - 32 + u) * 128];
+                        }
+                        const int cl0 = c0 - col0;
+                        tm_ld32(tb + cl0, yv);
+#pragma unroll
+                        for (int u = 31; u >= 0; --u) {
+                            const float rr = R[u], cr_ = f_t[cl0 + u].z * rr;
+                            const float yn = fmaf(-cr_, yp, yv[u] * rr);
+                            yp = (c0 + u < M) ? yn : yp;   // uniform
+                            yv[u] = yn;
+                        }
+                        tm_st32_nw(tb + cl0, yv);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) R[u] = Rn[u];
+                    }
+                }
+                tm_wait_st();
+                if (!gwait(bar_cv, ph_cv, false)) { failed = true; break; }
+                cv_pend = false;
+                // meeting rows h-1 (rank 0's last) and h (rank 1's first), in
+                // FP64 from both halves' values at their own scales:
+                // x_t = y'_t + (1-e_t) x_u, x_u = y''_u + (1-f_u) x_t
+                const float mine_c = cvs[(rank == 0 ? NH - 1 : 0) * 128 + p];
+                float4 in;
+                if (!exchange(make_float4(yp, mine_c, __int_as_float(ks), 0.f), in)) { failed = true; break; }
+                const int ks_peer = __float_as_int(in.z);
+                const double yt = rank == 0 ? ldexp((double)yp, -ks) : ldexp((double)in.x, -ks_peer);
+                const double yu = rank == 0 ? ldexp((double)in.x, -ks_peer) : ldexp((double)yp, -ks);
+                const double et = rank == 0 ? (double)mine_c : (double)in.y;
+                const double fu = rank == 0 ? (double)in.y : (double)mine_c;
+                const double xtd = (yt + (1.0 - et) * yu) / ((et + fu) - et * fu);
+                const double xud = yu + (1.0 - fu) * xtd;
+                if (rank == 0) {
+                    float xn = (float)ldexp(xtd, ks);   // x_{j+1} while sweeping up
+                    for (int c0 = NH - 32; c0 >= 0; c0 -= 32) {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) Rn[u] = cvs[(c0 + u) * 128 + p];
+                        tm_ld32(tb + c0, yv);
+#pragma unroll
+                        for (int u = 31; u >= 0; --u) {
+                            float xv = yv[u] + (1.0f - Rn[u]) * xn;
+                            xv = (c0 + u == NH - 1) ? xn : xv;
+                            xn = xv;
+                            yv[u] = live ? xv : 0.f;
+                            xmax = fmaxf(xmax, fabsf(yv[u]));
+                        }
+                        tm_st32_nw(tb + c0, yv);
+                    }
+                } else {
+                    float xpv = (float)ldexp(xud, ks);  // x_{j-1} while sweeping down
+                    for (int c0 = 0; c0 < NH; c0 += 32) {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) Rn[u] = cvs[(c0 + u) * 128 + p];
+                        tm_ld32(tb + c0, yv);
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) {
+                            float xv = yv[u] + (1.0f - Rn[u]) * xpv;
+                            xv = (c0 + u == 0) ? xpv : xv;
+                            xpv = xv;
+                            yv[u] = (live && col0 + c0 + u < M) ? xv : 0.f;
+                            xmax = fmaxf(xmax, fabsf(yv[u]));
+                        }
+                        tm_st32_nw(tb + c0, yv);
+                    }
+                }
+                tm_wait_st();
+            }
+            const int k2 = pow2_exp(group_max(xmax));
+            const float s2 = ldexpf(1.0f, k2);
+            // ---- TMEM w -> B tile (row j, K index p), FP16 hi/lo
+            for (int c0 = 0; c0 < NH; c0 += 32) {
+                float v[32];
+                tm_ld32(tb + c0, v);
+#pragma unroll
+                for (int u = 0; u < 32; ++u) v[u] *= s2;
+                split_rows32(sBh, sBl, v, c0, kq, lane, NH);
+            }
+            fence_proxy_async();
+            tc_fence_before();
+            gbar();
+            // ---- Q w (delta times d) into TMEM cols [acc, acc + NH): the resident tile, transposed
+            if (gt == 0) gemm_issue(tmem + acc, sA, sBh, NH, idesc, bar_mma, true);
+            mma_pend = true;
+            if (!gwait(bar_mma, ph_mma, false)) { failed = true; break; }
+            mma_pend = false;
+            tc_fence_after();
+            const int eun = -(24 + k1 + k2);            // this solve's result is 2^eun times the columns
+            const double unscale = ldexp(1.0, eun);
+            if (it + 1 < nit) {
+                // x0 stays in tensor memory columns [G, G + NH); its edge column
+                // goes to the peer for the correction residual
+                u0 = unscale;
+                eu0 = eun;
+                float te;
+                tm_ld1_nw(tmem + lane_base + G + (uint32_t)(rank == 0 ? NH - 1 : 0), te);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" : "+f"(te)::"memory");
+                float4 in;
+                if (!exchange(make_float4(te, 0.f, __int_as_float(eu0), 0.f), in)) { failed = true; break; }
+                edge_in = ldexp((double)in.x, __float_as_int(in.z) - eu0);
+                continue;
+            }
+            // ---- X = x0 + delta (FP64), staged as 16-column tiles (128-byte
+            // swizzle) and written by the copy engine as rows 0..KMAX-2 (the
+            // boundary row is not written); column M carries X's own value back
+            double sd = 0.0, sx = 0.0;
+            const double uk = unscale * ek, u0k = u0 * ek;     // this row's 1/d_k
+            float dv[16], xv[16];
+            tm_ld16_nw(tmem + lane_base + acc, dv);
+            tm_ld16_nw(tmem + lane_base + G, xv);   // x0 (unused after a single solve)
+            for (int c = 0; c < nch; ++c) {
+                const int c0 = 16 * c;
+                uint8_t *slot = sB + (c % kPairStage) * kPairTileB;
+                tm_wait_ld32(dv, xv);
+                double xn[16];
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    const int j = col0 + c0 + u;
+                    const double dl = (double)dv[u] * uk;
+                    xn[u] = (res_x ? (double)xv[u] * u0k : 0.0) + dl;
+                    if (kq < NZ && j < M) {
+                        sd += dl * dl;
+                        sx += xn[u] * xn[u];
+                    }
+                    if (j == M) xn[u] = ym_keep;        // column M (uniform in the warp)
+                }
+#pragma unroll
+                for (int u = 0; u < 16; u += 2)
+                    *reinterpret_cast<double2 *>(slot + kq * 128 + (((u >> 1) ^ (kq & 7)) << 4)) =
+                        make_double2(xn[u], xn[u + 1]);
+                fence_proxy_async();
+                if (gt == 0) bulk_wait_read<kPairStage - 2>();   // the slot's previous store has read it
+                gbar();
+                if (c + 1 < nch) {
+                    tm_ld16_nw(tmem + lane_base + acc + c0 + 16, dv);
+                    tm_ld16_nw(tmem + lane_base + G + c0 + 16, xv);
+                }
+                if (gt == 0 && col0 + c0 < J) {
+                    tma_store_2d(&tm_xs, col0 + c0, row0, slot);
+                    bulk_commit();
+                }
+            }
+            if (gt == 0) bulk_wait_all();               // tiles written, staging free for the next item
+            // per-half sums (the host adds the two halves)
+            sd = warp_sum(sd);
+            sx = warp_sum(sx);
+            double sq = warp_sum((double)sxf * ek * ek);
+            gbar();
+            if (lane == 0) { d_red[warp & 3] = sd; d_red[8 + (warp & 3)] = sx; d_red[16 + (warp & 3)] = sq; }
+            gbar();
+            if (gt == 0) {
+                double a = 0.0, bb = 0.0, q = 0.0;
+                for (int i = 0; i < 4; ++i) { a += d_red[i]; bb += d_red[8 + i]; q += d_red[16 + i]; }
+                if (res_x) {                            // the first solve's delta is x0 itself
+                    cr[0] = q * u0 * u0;
+                    cr[1] = q * u0 * u0;
+                }
+                cr[2 * it] = a;
+                cr[2 * it + 1] = bb;
+            }
+            gbar();
+        }
+    }
+    if (!stag_sent && gt == 0) mbar_arrive(bar_stagger);
+    // drain this group's copies and products still in flight (bounded)
+    for (int sl = 0; sl < kPairRing; ++sl)
+        if (ring_pend & (1u << sl)) mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u);
+    if (cv_pend) mbar_wait(bar_cv, ph_cv);
+    if (mma_pend) mbar_wait(bar_mma, ph_mma);
+    if (failed) {
+        // this half of every mode the group left unsolved becomes NaN
+        if (gt == 0) {
+            bulk_wait_all();
+            atomicExch(x.err, 1);
+        }
+        gbar();
+        const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+        for (long long item = fail_item; item < items; item += stride) {
+            const int o = (int)(item / nb), b = (int)(item % nb);
+            const int l = (o & 1) ? (o >> 1) + t.N : (o >> 1);
+            double *Xl = w.X + (size_t)b * w.sX + (size_t)l * K * J;
+            for (int i = gt; i < NZ * NH; i += 128) {
+                const int kk = i / NH, j = col0 + i % NH;
+                if (j < M) Xl[(size_t)kk * J + j] = qnan;
+            }
+        }
+    }
+    if (tid == 0 && a_inflight) mbar_wait(bar_a, 0);
+    tc_fence_before();
+    __syncthreads();
+    // no peer writes into this CTA's shared memory after this point
+    cluster_sync_all();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+}
+
+// ---------------------------------------------------------------------------
 // Wide pipeline: grids whose radial extent does not fit one CTA's tiles
 // (JMAX > 256, e.g. the 512 x 128 x 512 serving class) or whose rows are not
 // 16-byte tiles (JMAX not a multiple of 16).  The same refinement as
@@ -1186,7 +1872,7 @@ constexpr int kWideMaxJ = 1024;  // largest JMAX of the wide pipeline
 constexpr int kWideTiles = kWideMaxJ / kWideN;
 
 template <bool kFirst>
-__global__ void __launch_bounds__(256) k_wide_resid(DevTables t, Work w, WideDev d, int nb)
+__global__ void __launch_bounds__(256) k_wide_resid(DevTables t, Work w, MixedDev x, WideDev d, int nb)
 {
     __shared__ float tile[32][129];
     __shared__ float red[8];
@@ -1221,7 +1907,7 @@ __global__ void __launch_bounds__(256) k_wide_resid(DevTables t, Work w, WideDev
                 if (j < M - 1) ax += cmj * xr[j + 1];
                 r = r - ax;
             }
-            v = (float)r;
+            v = (float)(x.zsc[k] * r);   // times d_k for the orthogonal transform
         }
         tile[tx][k] = v;
         vmax = fmaxf(vmax, fabsf(v));
@@ -1243,11 +1929,12 @@ __global__ void __launch_bounds__(256) k_wide_resid(DevTables t, Work w, WideDev
 }
 
 // out[item][j][row] = sum_k A(row, k) in[item][j][k] for one 256-column tile:
-// A is the plan's 2^12-scaled FP16 hi/lo image of U or V, the input tile is
-// scaled by a power of two from its maximum and split to FP16 hi/lo in
-// shared memory, three MMA passes accumulate in FP32 in tensor memory.
+// A is the plan's 2^12-scaled FP16 hi/lo image of Q^T, or with trans its
+// transpose Q; the input tile is scaled by a power of two from its maximum
+// and split to FP16 hi/lo in shared memory, three MMA passes accumulate in
+// FP32 in tensor memory.
 __global__ void __launch_bounds__(256, 1) k_wide_gemm(const uint8_t *aimg, const float *in, float *out,
-                                                      const unsigned *tmax, WideDev d, int *err)
+                                                      const unsigned *tmax, WideDev d, int trans, int *err)
 {
     extern __shared__ __align__(1024) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1291,7 +1978,7 @@ __global__ void __launch_bounds__(256, 1) k_wide_gemm(const uint8_t *aimg, const
     __syncthreads();
     a_ok = *flag == 0;
     const uint32_t idesc = (1u << 4) | ((uint32_t)(kWideN >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-    if (a_ok && tid == 0) gemm_issue(tmem, sA, sBh, kWideN, idesc, &bars[0]);
+    if (a_ok && tid == 0) gemm_issue(tmem, sA, sBh, kWideN, idesc, &bars[0], trans != 0);
     bool d_ok = a_ok && mbar_wait(&bars[0], 0);
     if (a_ok && !d_ok) *flag = 1;
     __syncthreads();
@@ -1415,7 +2102,7 @@ __global__ void __launch_bounds__(256) k_wide_update(DevTables t, Work w, MixedD
         for (int e = threadIdx.x; e < 32 * NZ; e += 256) {
             const int k = e >> 5, jj = e & 31, j = j0 + jj;
             if (j < M) {
-                const double dl = (double)tile[k][jj];
+                const double dl = (double)tile[k][jj] * x.zsc[128 + k];   // Q w / d_k
                 const size_t o = (size_t)k * J + j;
                 const double xn = (it > 0 ? xl[o] : 0.0) + dl;
                 if (last) Xl[o] = xn;
@@ -1505,52 +2192,69 @@ std::vector<float> chy::mixed_sweep_table(const chy::HostPlan &hp)
     return t;
 }
 
+// Per vertical row k (128, padding rows 1, 1, 0, 0): d_k, 1/d_k,
+// d_k AN_k / d_(k-1) and d_k CN_k / d_(k+1), with D = diag(d) the symmetriser
+// of T_z (U = Q^T D, V = D^-1 Q).
+std::vector<double> chy::mixed_row_scales(const chy::HostPlan &hp)
+{
+    const int NZ = hp.NZ;
+    std::vector<double> z(4 * 128, 0.0);
+    for (int k = 0; k < 128; ++k) z[k] = z[128 + k] = 1.0;
+    for (int k = 0; k < NZ; ++k) {
+        z[k] = hp.dsc[k];
+        z[128 + k] = 1.0 / hp.dsc[k];
+    }
+    for (int k = 0; k < NZ; ++k) {
+        z[256 + k] = k > 0 ? hp.dsc[k] * hp.an[k] / hp.dsc[k - 1] : 0.0;
+        z[384 + k] = k + 1 < NZ ? hp.dsc[k] * hp.cn[k] / hp.dsc[k + 1] : 0.0;
+    }
+    return z;
+}
+
 size_t chy_mixed_pack_tables(const chy::HostPlan *hp, std::vector<char> *image, bool mixed)
 {
     if (!mixed) return image->size();
-    // [U hi | U lo | V hi | V lo]: K-major swizzled FP16 tiles of 2^12 * U(p,k)
-    // (rows p, K index k) and 2^12 * V(k,p) (rows k, K index p)
-    std::vector<uint8_t> img((size_t)2 * kAImg, 0);
+    // [Q^T hi | Q^T lo]: a K-major swizzled FP16 tile of 2^12 * Q(k,p) (rows p,
+    // K index k); read through the MN-major descriptor it is 2^12 * Q
+    std::vector<uint8_t> img((size_t)kAImg, 0);
     const int NZ = hp->NZ;
-    auto put = [&](size_t base, int row, int k, double v) {
-        v *= (double)kAScale;
-        const __half h = __double2half(v);
-        const __half l = __double2half(v - (double)__half2float(h));
-        const uint32_t o = kmaj_off(row, k, kTiles);
-        std::memcpy(&img[base + o], &h, 2);
-        std::memcpy(&img[base + kTiles * kTiles * 2 + o], &l, 2);
-    };
     for (int p = 0; p < NZ; ++p)
         for (int k = 0; k < NZ; ++k) {
-            put(0, p, k, hp->U[(size_t)p * NZ + k]);
-            put(kAImg, k, p, hp->V[(size_t)k * NZ + p]);
+            const double v = (double)kAScale * hp->Qt[(size_t)p * NZ + k];
+            const __half h = __double2half(v);
+            const __half l = __double2half(v - (double)__half2float(h));
+            const uint32_t o = kmaj_off(p, k, kTiles);
+            std::memcpy(&img[o], &h, 2);
+            std::memcpy(&img[kTiles * kTiles * 2 + o], &l, 2);
         }
     size_t off = (image->size() + 1023) & ~(size_t)1023;
     image->resize(off + img.size());
     std::memcpy(image->data() + off, img.data(), img.size());
     // eigenvalues as FP32, padded with -1 (any nonzero diagonal works for the
-    // zero padding rows)
+    // zero padding rows), then the row scales, then the sweep table, each at
+    // the next 256-byte boundary
     std::vector<float> lam(128, -1.0f);
     for (int p = 0; p < NZ; ++p) lam[p] = (float)hp->lam[p];
-    size_t off2 = (image->size() + 255) & ~(size_t)255;
-    image->resize(off2 + lam.size() * sizeof(float));
-    std::memcpy(image->data() + off2, lam.data(), lam.size() * sizeof(float));
-    // radial sweep coefficients, then the sweep table at the next 256-byte
-    // boundary
+    auto append = [&](const void *src, size_t bytes) {
+        const size_t o = (image->size() + 255) & ~(size_t)255;
+        image->resize(o + bytes);
+        std::memcpy(image->data() + o, src, bytes);
+    };
+    append(lam.data(), lam.size() * sizeof(float));
+    const std::vector<double> zsc = chy::mixed_row_scales(*hp);
+    append(zsc.data(), zsc.size() * sizeof(double));
     const std::vector<float> sw = chy::mixed_sweep_table(*hp);
-    size_t off3 = (image->size() + 255) & ~(size_t)255;
-    image->resize(off3 + sw.size() * sizeof(float));
-    std::memcpy(image->data() + off3, sw.data(), sw.size() * sizeof(float));
-    return off;   // lam and the sweep table follow at 256-byte boundaries
+    append(sw.data(), sw.size() * sizeof(float));
+    return off;
 }
 
 std::vector<double> chy::mixed_operand_tiles(const chy::HostPlan &hp)
 {
     std::vector<char> image;
     const size_t off = chy_mixed_pack_tables(&hp, &image, true);
-    std::vector<double> out((size_t)4 * kTiles * kTiles);
-    for (int t = 0; t < 4; ++t) {
-        const size_t base = off + (size_t)(t >> 1) * kAImg + (size_t)(t & 1) * kTiles * kTiles * 2;
+    std::vector<double> out((size_t)2 * kTiles * kTiles);
+    for (int t = 0; t < 2; ++t) {
+        const size_t base = off + (size_t)t * kTiles * kTiles * 2;
         for (int r = 0; r < kTiles; ++r)
             for (int k = 0; k < kTiles; ++k) {
                 __half h;
@@ -1566,9 +2270,11 @@ void chy_mixed_bind_tables(chy_plan *p, char *dev_base)
     if (!p->mx) p->mx = new MixedState();
     if (p->precision != CHY_PREC_MIXED) return;   // no mixed tables packed
     p->mx->dev.aimg = reinterpret_cast<const uint8_t *>(dev_base);
-    size_t lam_off = (((size_t)(dev_base - p->d_tables) + 2 * kAImg) + 255) & ~(size_t)255;
+    const size_t lam_off = (((size_t)(dev_base - p->d_tables) + kAImg) + 255) & ~(size_t)255;
     p->mx->dev.lam = reinterpret_cast<const float *>(p->d_tables + lam_off);
-    const size_t sw_off = (lam_off + 128 * sizeof(float) + 255) & ~(size_t)255;
+    const size_t zsc_off = (lam_off + 128 * sizeof(float) + 255) & ~(size_t)255;
+    p->mx->dev.zsc = reinterpret_cast<const double *>(p->d_tables + zsc_off);
+    const size_t sw_off = (zsc_off + 4 * 128 * sizeof(double) + 255) & ~(size_t)255;
     p->mx->dev.sw_mul = reinterpret_cast<const float *>(p->d_tables + sw_off);
     p->mx->dev.sw_piv = p->mx->dev.sw_mul + (size_t)(p->hp.N + 1) * round64(p->hp.J) * 128;
 }
@@ -1656,11 +2362,11 @@ static int wide_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
         if (cudaMemsetAsync(d.rmax, 0, mb, s) != cudaSuccess || cudaMemsetAsync(d.wmax, 0, mb, s) != cudaSuccess)
             return CHY_ERR_CUDA;
         const dim3 rg(d.Jt / 32, items), gg(d.nt, items);
-        if (it == 0) k_wide_resid<true><<<rg, 256, 0, s>>>(t, p->w, d, nb);
-        else k_wide_resid<false><<<rg, 256, 0, s>>>(t, p->w, d, nb);
-        k_wide_gemm<<<gg, 256, gsm, s>>>(x.aimg, d.R, d.O, d.rmax, d, x.err);
+        if (it == 0) k_wide_resid<true><<<rg, 256, 0, s>>>(t, p->w, x, d, nb);
+        else k_wide_resid<false><<<rg, 256, 0, s>>>(t, p->w, x, d, nb);
+        k_wide_gemm<<<gg, 256, gsm, s>>>(x.aimg, d.R, d.O, d.rmax, d, 0, x.err);
         k_wide_sweep<<<items, 128, 2 * t.M * sizeof(float), s>>>(t, x, d);
-        k_wide_gemm<<<gg, 256, gsm, s>>>(x.aimg + kAImg, d.R, d.O, d.wmax, d, x.err);
+        k_wide_gemm<<<gg, 256, gsm, s>>>(x.aimg, d.R, d.O, d.wmax, d, 1, x.err);
         k_wide_update<<<items, 256, 0, s>>>(t, p->w, x, d, it, it == nit - 1 ? 1 : 0);
         if (cudaGetLastError() != cudaSuccess) return CHY_ERR_CUDA;
     }
@@ -1683,11 +2389,57 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
     const size_t sm = MixedSmem::bytes(d.ntile);
     // two approximate solves (one correction) keep the iterate in tensor memory
     if (d.nit <= 2 && !p->mx->tm_ok) return CHY_ERR_CUDA;   // tensor map over X not encoded
+    const long long items = (long long)nb * p->hp.L;
+    const int cap = p->mode_ctas > 0 && p->mode_ctas < p->num_sms ? p->mode_ctas : p->num_sms;
+    if (d.nit <= 2 && p->mode_kernel == 0) {
+        // CTA pairs, two items per CTA
+        MixedState &ms = *p->mx;
+        if (ms.pair_clusters < 0) {
+            ms.pair_clusters = 0;
+            if (ensure_smem((const void *)k_mode_pair, PairSmem::bytes) == cudaSuccess) {
+                cudaLaunchConfig_t cfg = {};
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = 2;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                cfg.gridDim = dim3(2 * (unsigned)p->num_sms, 1, 1);
+                cfg.blockDim = dim3(256, 1, 1);
+                cfg.dynamicSmemBytes = PairSmem::bytes;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                int n = 0;
+                if (cudaOccupancyMaxActiveClusters(&n, (const void *)k_mode_pair, &cfg) == cudaSuccess) ms.pair_clusters = n;
+                cudaGetLastError();
+            }
+        }
+        if (ms.pair_clusters > 0) {
+            long long pairs = (items + 1) / 2;
+            pairs = std::min<long long>(pairs, ms.pair_clusters);
+            pairs = std::min<long long>(pairs, std::max(1, cap / 2));
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = 2;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(2 * (unsigned)pairs, 1, 1);
+            cfg.blockDim = dim3(256, 1, 1);
+            cfg.dynamicSmemBytes = PairSmem::bytes;
+            cfg.stream = s;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            if (cudaLaunchKernelEx(&cfg, k_mode_pair, p->t, p->w, d, nb, p->mx->tm_x, p->mx->tm_xs) != cudaSuccess)
+                return CHY_ERR_CUDA;
+            ms.paired = true;
+            *launches = 1;
+            return CHY_OK;
+        }
+    }
+    p->mx->paired = false;
     const void *kern = d.nit <= 2 ? (const void *)k_mode_mixed<true> : (const void *)k_mode_mixed<false>;
     cudaError_t e = ensure_smem(kern, sm);
     if (e != cudaSuccess) return CHY_ERR_CUDA;
-    const long long items = (long long)nb * p->hp.L;
-    const int cap = p->mode_ctas > 0 && p->mode_ctas < p->num_sms ? p->mode_ctas : p->num_sms;
     const int grid = (int)(items < cap ? items : cap);
     if (d.nit <= 2) k_mode_mixed<true><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x, p->mx->tm_xs);
     else k_mode_mixed<false><<<grid, 256, sm, s>>>(p->t, p->w, d, nb, p->mx->tm_x, p->mx->tm_xs);
@@ -1726,6 +2478,13 @@ int *chy_mixed_host_error_word(chy_plan *p)
     return (p->precision == CHY_PREC_MIXED && p->mx) ? p->mx->h_err : nullptr;
 }
 
+int chy_mixed_last_kernel(const chy_plan *p)
+{
+    if (p->precision != CHY_PREC_MIXED || !p->mx) return 0;
+    if (p->mx->is_wide) return 3;
+    return p->mx->paired ? 2 : 1;
+}
+
 int chy_dbg_mixed_probe_set(chy_plan *p, int polls)
 {
     if (p->precision != CHY_PREC_MIXED || !p->mx || polls < 0) return CHY_ERR_ARG;
@@ -1740,11 +2499,17 @@ void chy_mixed_fill_diag(const chy_plan *p, int slot, chy_diag *d)
     const int nit = std::min(1 + p->refine, 8);
     const double *c = p->mx->h_corr + (size_t)slot * p->mx->dev.scorr;
     d->iterations = nit;
+    // k_mode_pair leaves one sum per radial half: [0, 4) and [8, 12)
+    const bool halves = p->mx->paired;
     for (int it = 0; it < nit && it < 8; ++it) {
         double sd = 0.0, sx = 0.0;
         for (int l = 0; l < p->hp.L; ++l) {
             sd += c[(size_t)l * 16 + 2 * it];
             sx += c[(size_t)l * 16 + 2 * it + 1];
+            if (halves) {
+                sd += c[(size_t)l * 16 + 8 + 2 * it];
+                sx += c[(size_t)l * 16 + 8 + 2 * it + 1];
+            }
         }
         d->corr_rel[it] = sx > 0.0 ? std::sqrt(sd / sx) : 0.0;
     }
@@ -1779,11 +2544,13 @@ void chy_mixed_release(chy_plan *p)
 }
 
 // ---------------------------------------------------------------------------
-// Self-test of the tensor-core path: D = (2^12 U) * Bm^T for one tile, where
-// Bm (NT x 128, row-major FP32) is split to FP16 hi/lo by the same code the
+// Self-test of the tensor-core path: D = (2^12 Q^T) * Bm^T for one tile (with
+// trans: 2^12 Q, the same tile through the transposed descriptor), where Bm
+// (NT x 128, row-major FP32) is split to FP16 hi/lo by the same code the
 // solver uses.  Writes D (128 x NT, row-major FP32).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1) k_umma_selftest(const uint8_t *aimg, const float *Bm, float *D, int NT, int *err)
+__global__ void __launch_bounds__(128, 1) k_umma_selftest(const uint8_t *aimg, const float *Bm, float *D, int NT,
+                                                          int trans, int *err)
 {
     extern __shared__ __align__(1024) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1816,7 +2583,7 @@ __global__ void __launch_bounds__(128, 1) k_umma_selftest(const uint8_t *aimg, c
     ok = mbar_wait(&bars[1], 0);
     __syncthreads();
     const uint32_t idesc = (1u << 4) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-    if (ok && tid == 0) gemm_issue(tmem, sA, sBh, NT, idesc, &bars[0]);
+    if (ok && tid == 0) gemm_issue(tmem, sA, sBh, NT, idesc, &bars[0], trans != 0);
     if (ok) ok = mbar_wait(&bars[0], 0);
     tc_fence_after();
     if (ok) {
@@ -1834,7 +2601,8 @@ __global__ void __launch_bounds__(128, 1) k_umma_selftest(const uint8_t *aimg, c
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
 }
 
-// Test hook: which = 0 uses the U tile, 1 the V tile of the plan.
+// Test hook: which = 0 multiplies by the plan's tile (2^12 Q^T), 1 by its
+// transpose (2^12 Q).
 extern "C" int chy_dbg_umma(chy_plan *p, int which, const float *Bm_dev, float *D_dev, int NT)
 {
     if (!p || !p->mx || !Bm_dev || !D_dev || NT < 64 || NT > 256 || NT % 64) return CHY_ERR_ARG;
@@ -1843,7 +2611,7 @@ extern "C" int chy_dbg_umma(chy_plan *p, int which, const float *Bm_dev, float *
     cudaMemset(err, 0, sizeof(int));
     const size_t sm = (size_t)kAImg + (size_t)NT * 512 + 64;
     ensure_smem((const void *)k_umma_selftest, sm);
-    k_umma_selftest<<<1, 128, sm>>>(p->mx->dev.aimg + (which ? kAImg : 0), Bm_dev, D_dev, NT, err);
+    k_umma_selftest<<<1, 128, sm>>>(p->mx->dev.aimg, Bm_dev, D_dev, NT, which ? 1 : 0, err);
     int h = 0;
     cudaError_t e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
     cudaFree(err);

@@ -732,6 +732,8 @@ int build_host_plan(const chy_grid &g, HostPlan &hp, std::string &err)
         hp.lam.resize(NZ);
         hp.U.assign((size_t)NZ * NZ, 0.0);
         hp.V.assign((size_t)NZ * NZ, 0.0);
+        hp.Qt.assign((size_t)NZ * NZ, 0.0);
+        hp.dsc = dsc;
         for (int p = 0; p < NZ; p++) {
             const int q = ord[p];
             hp.lam[p] = dd[q];
@@ -739,6 +741,7 @@ int build_host_plan(const chy_grid &g, HostPlan &hp, std::string &err)
                 const double qk = zz[k + (size_t)NZ * q];
                 hp.V[(size_t)k * NZ + p] = qk / dsc[k];   // V(k,p)
                 hp.U[(size_t)p * NZ + k] = qk * dsc[k];   // U(p,k)
+                hp.Qt[(size_t)p * NZ + k] = qk;           // Q(k,p)
             }
         }
     }

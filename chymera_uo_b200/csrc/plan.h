@@ -95,8 +95,10 @@ struct HostPlan {
     double cmmax = 0, ammin = 0, cnmax = 0;
     std::vector<double> xlamm;               // cos(m*dtheta), m = 0..N
 
-    // vertical eigenbasis: T_z = V diag(lam) U, U = V^-1; row-major [NZ][NZ]
-    std::vector<double> lam, U, V;
+    // vertical eigenbasis: T_z = V diag(lam) U, U = V^-1; row-major [NZ][NZ].
+    // U = Q^T D and V = D^-1 Q with Q orthogonal (Qt = Q^T, row-major
+    // [p][k]) and D = diag(dsc) the symmetriser of T_z
+    std::vector<double> lam, U, V, Qt, dsc;
 
     // ZAXPHI abscissae X(1..NPOINT)
     int npoint = 8;
@@ -115,8 +117,11 @@ int tridiag_eigen(int n, double *d, double *e, double *z);
 // The mixed path's radial sweep table of a grid (k_mixed.cu): two FP32
 // planes [N+1][64 ceil(JMAX/64)][128], multipliers then pivot reciprocals.
 std::vector<float> mixed_sweep_table(const HostPlan &hp);
-// Its eigenbasis operand tiles read back through their swizzled layout:
-// [U hi, U lo, V hi, V lo], each [128 rows][128 K] (test hook).
+// Its eigenbasis operand tile read back through its swizzled layout:
+// [Q^T hi, Q^T lo], each [128 rows][128 K] (test hook).
 std::vector<double> mixed_operand_tiles(const HostPlan &hp);
+// Its per-row scales [4][128]: d_k, 1/d_k, d_k AN_k / d_(k-1),
+// d_k CN_k / d_(k+1).
+std::vector<double> mixed_row_scales(const HostPlan &hp);
 
 }  // namespace chy

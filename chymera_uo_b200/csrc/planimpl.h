@@ -24,6 +24,7 @@ struct chy_plan {
     int device = 0;                // the device the plan's tables and work space live on
     // launch schedule (chy_autotune_multi picks these; 0 = the default)
     int mode_ctas = 0;             // persistent CTAs of the fused mixed mode solve (default: one per SM)
+    int mode_kernel = 0;           // fused mixed mode solve: 0 CTA pairs (k_mode_pair), 1 one CTA per item
     int blk_warps = 8;             // BLKTRI order: warps per CTA (4, 8, 16)
     int blk_ctas_per_sm = 2;       // BLKTRI order: CTAs per SM (blk_warps * this <= 16)
     int chunk = 0;                 // chy_solve_multi: solves per launch sequence (default max_batch)
@@ -124,6 +125,9 @@ int chy_mixed_read_error(chy_plan *p, int *host_word, cudaStream_t s);
 // The plan's own pinned error word (mixed plans), else null.
 int *chy_mixed_host_error_word(chy_plan *p);
 // Test hook behind chy_dbg_mixed_probe.
+// The kernel of the plan's last mixed mode solve: 0 none / not mixed, 1 k_mode_mixed,
+// 2 k_mode_pair, 3 the wide pipeline.
+int chy_mixed_last_kernel(const chy_plan *p);
 int chy_dbg_mixed_probe_set(chy_plan *p, int polls);
 // Allocates the FP64 iterate used when two or more corrections are set.
 int chy_mixed_ensure_iterate(chy_plan *p);

@@ -145,6 +145,10 @@ int chy_solve_multi(int n, chy_plan *const *plans, const double *const *rho, dou
  *   chunk        solves per launch sequence (max_batch, /2, /4);
  *   mode_ctas    persistent CTAs of each fused mixed mode solve (all SMs, 1/2,
  *                1/4: grids running side by side then share the SMs);
+ *   mode_kernel  not searched (the two kernels round the mixed result
+ *                differently, within the same tolerance): the plan's own
+ *                setting, 0 = CTA pairs holding two (solve, mode) items per
+ *                SM (default), 1 = one CTA per item;
  *   blk_warps,   the BLKTRI-order path's stage schedule: warps per CTA (the
  *   blk_ctas_per_sm  cyclic-reduction tasks of a stage in flight at once) and
  *                CTAs per SM.
@@ -153,15 +157,15 @@ int chy_solve_multi(int n, chy_plan *const *plans, const double *const *rho, dou
  * `stream`.  The call synchronises `stream`; make it before any capture.  The
  * results of the last call are in phi. */
 typedef struct chy_tune {
-    int streams, chunk, mode_ctas, blk_warps, blk_ctas_per_sm;
+    int streams, chunk, mode_ctas, blk_warps, blk_ctas_per_sm, mode_kernel;
     double ms;           /* one chy_solve_multi call under the chosen schedule */
     double ms_default;   /* the same under the default schedule              */
     int candidates;      /* schedules timed                                   */
 } chy_tune;
 int chy_autotune_multi(int n, chy_plan *const *plans, const double *const *rho, double *const *phi, void *stream,
                        int repeats, chy_tune *out);
-/* A plan's launch schedule (the first five fields of chy_tune; 0 = default
- * for streams, chunk and mode_ctas), e.g. to reuse a tuned schedule in a
+/* A plan's launch schedule (the first six fields of chy_tune; 0 = default
+ * for streams, chunk, mode_ctas and mode_kernel), e.g. to reuse a tuned schedule in a
  * later run.  The timing fields are ignored / returned as 0. */
 int chy_plan_set_schedule(chy_plan *p, const chy_tune *c);
 int chy_plan_get_schedule(const chy_plan *p, chy_tune *c);

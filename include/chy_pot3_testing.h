@@ -38,8 +38,10 @@ int chy_dbg_blktri(const chy_grid *g, int l, double *y);
 long long chy_dbg_work(chy_plan *p, const char *name, double *out, long long cap);
 
 /* One tensor-core tile product of a CHY_PREC_MIXED plan:
- * D(128 x nt) = 4096 * U_pad(128 x 128) * Bm(nt x 128)^T with U split into
- * FP16 hi/lo parts exactly as the mode solve uses it (which = 0: U, 1: V).
+ * D(128 x nt) = 4096 * A_pad(128 x 128) * Bm(nt x 128)^T with A the plan's
+ * orthogonal vertical eigenbasis split into FP16 hi/lo parts exactly as the
+ * mode solve uses it: which = 0 reads the tile as Q^T (K-major descriptor),
+ * 1 as Q (the same tile through the transposed, MN-major descriptor).
  * Bm and D are device pointers (FP32, row-major); nt is 64, 128, 192 or 256.
  * Returns a CHY_* status after synchronising the device. */
 int chy_dbg_umma(chy_plan *p, int which, const float *Bm_dev, float *D_dev, int nt);
@@ -50,6 +52,11 @@ int chy_dbg_umma(chy_plan *p, int which, const float *Bm_dev, float *D_dev, int 
  * out, the CTA poisons its modes with NaN, sets the device error word and
  * exits, and the solve reports CHY_ERR_TIMEOUT.  0 switches it off. */
 int chy_dbg_mixed_probe(chy_plan *p, int polls);
+
+/* The kernel that ran the plan's last mixed mode solve: 1 k_mode_mixed (one
+ * CTA per mode), 2 k_mode_pair (CTA pairs), 3 the wide pipeline, 0 none yet or
+ * not a CHY_PREC_MIXED plan; -CHY_ERR_ARG for a null plan. */
+int chy_dbg_mixed_kernel(const chy_plan *p);
 
 #ifdef __cplusplus
 }

@@ -77,6 +77,31 @@ def test_mixed_meets_1e10(chylib, cfg):
     assert d["iterations"] >= 1 and d["corr_rel"][0] == pytest.approx(1.0)
 
 
+@pytest.mark.parametrize("J,K,L", [(256, 128, 64), (64, 32, 64), (80, 32, 64), (192, 64, 32)])
+def test_mixed_mode_kernels(chylib, J, K, L):
+    """Both fused mode-solve kernels meet 1e-10 against the oracle: the
+    default k_mode_pair (a CTA pair per mode, two modes per SM, the sweeps'
+    meeting rows and the iterate's edge column exchanged through distributed
+    shared memory) and k_mode_mixed (one CTA per mode, mode_kernel = 1).
+    Each is deterministic: a mode's result does not depend on the batch
+    around it or on which CTAs solved it."""
+    rho, ref, _, _ = oracle_result((J, K, L), seed_override=17)
+    rho2 = synth.disk_density(J, K, L, 18, spiral=True, spectrum=True)
+    ws = write_set(J, K)
+    outs = {}
+    for mk, kernel in ((0, 2), (1, 1)):
+        plan = chylib.Plan(chylib.grid(J, K, L), "mixed", 3)
+        plan.set_schedule(mode_kernel=mk)
+        (single,), (d,) = plan.solve_batch([rho], diag=True)
+        assert chylib.lib().chy_dbg_mixed_kernel(plan._p) == kernel
+        assert rel_l2(single[ws], ref[ws]) < 1e-10
+        assert d["iterations"] == 2 and d["corr_rel"][0] == pytest.approx(1.0) and d["corr_rel"][1] < 1e-5
+        batch = plan.solve_batch([rho, rho2, rho])
+        assert np.array_equal(batch[0], single) and np.array_equal(batch[2], single)
+        outs[mk] = single
+    assert rel_l2(outs[0][ws], outs[1][ws]) < 1e-10
+
+
 def test_mixed_refinement_converges_geometrically(chylib):
     rho, ref, _, _ = oracle_result(3)
     ws = write_set(256, 128)
@@ -246,7 +271,9 @@ def test_coef_diagnostics(chylib):
 
 
 def test_tensor_core_tile_product(chylib):
-    """One tcgen05 tile product (FP16 hi/lo, three passes) against FP64."""
+    """One tcgen05 tile product (FP16 hi/lo, three passes) against FP64, with
+    the plan's resident eigenbasis tile read as Q^T (K-major descriptor) and
+    as Q (the transposed, MN-major descriptor)."""
     import ctypes as C
     import torch
     J, K, L = 256, 128, 256
@@ -254,17 +281,18 @@ def test_tensor_core_tile_product(chylib):
     plan = chylib.Plan(g, "mixed", 1)
     NZ = K - 1
     out = np.zeros(NZ * NZ)
-    chylib.lib().chy_dbg_table(C.byref(g), b"U", out.ctypes.data_as(C.POINTER(C.c_double)), NZ * NZ)
-    U = out.reshape(NZ, NZ)
-    for NT in (64, 256):
-        Bm = np.zeros((NT, 128), np.float32)
-        Bm[:, :NZ] = np.random.default_rng(NT).uniform(-2000, 2000, (NT, NZ))
-        Bd = torch.from_numpy(Bm).cuda()
-        Dd = torch.zeros((128, NT), dtype=torch.float32, device="cuda")
-        assert chylib.lib().chy_dbg_umma(plan._p, 0, Bd.data_ptr(), Dd.data_ptr(), NT) == 0
-        ref = np.zeros((128, 128)); ref[:NZ, :NZ] = U
-        ref = 4096.0 * ref @ Bm.astype(np.float64).T
-        assert np.abs(Dd.cpu().numpy() - ref).max() <= 5e-6 * np.abs(ref).max()
+    chylib.lib().chy_dbg_table(C.byref(g), b"Qt", out.ctypes.data_as(C.POINTER(C.c_double)), NZ * NZ)
+    Qt = out.reshape(NZ, NZ)
+    for which, A in ((0, Qt), (1, Qt.T)):
+        for NT in (64, 256):
+            Bm = np.zeros((NT, 128), np.float32)
+            Bm[:, :NZ] = np.random.default_rng(NT).uniform(-2000, 2000, (NT, NZ))
+            Bd = torch.from_numpy(Bm).cuda()
+            Dd = torch.zeros((128, NT), dtype=torch.float32, device="cuda")
+            assert chylib.lib().chy_dbg_umma(plan._p, which, Bd.data_ptr(), Dd.data_ptr(), NT) == 0
+            ref = np.zeros((128, 128)); ref[:NZ, :NZ] = A
+            ref = 4096.0 * ref @ Bm.astype(np.float64).T
+            assert np.abs(Dd.cpu().numpy() - ref).max() <= 5e-6 * np.abs(ref).max(), (which, NT)
 
 
 def test_status_codes_on_device(chylib):

@@ -120,26 +120,47 @@ def test_mixed_sweep_table_is_the_two_sided_elimination(chylib, J, K, L):
 
 
 @pytest.mark.parametrize("J,K,L", [(64, 32, 64), (128, 128, 64)])
-def test_mixed_operand_tiles_are_hi_lo_splits(chylib, J, K, L):
-    """The eigenbasis operands of the tensor-core products, read back through
-    their K-major 128-byte-swizzled layout: hi = fp16(2^12 U(p,k)) and
-    lo = fp16(2^12 U(p,k) - hi) with rows p and K index k, the same for
-    V(k,p) with rows k and K index p, zero outside NZ x NZ; hi + lo carries
-    2^12 U to about 22 bits."""
+def test_mixed_row_scales_symmetrise_the_vertical_operator(chylib, J, K, L):
+    """U = Q^T D and V = D^-1 Q with Q orthogonal; the row scales carry d_k,
+    1/d_k and the vertical stencil coefficients conjugated by D
+    (d_k AN_k / d_(k-1), d_k CN_k / d_(k+1))."""
     g = chylib.grid(J, K, L)
     NZ = K - 1
-    tiles = table(chylib, g, "umma_tiles", 4 * 128 * 128).reshape(4, 128, 128)
-    U = table(chylib, g, "U", NZ * NZ).reshape(NZ, NZ)   # U[p][k]
-    V = table(chylib, g, "V", NZ * NZ).reshape(NZ, NZ)   # V[k][p]
-    for t, A in ((0, U), (2, V)):
-        v = 4096.0 * A
-        hi = v.astype(np.float16).astype(np.float64)
-        lo = (v - hi).astype(np.float16).astype(np.float64)
-        assert np.array_equal(tiles[t, :NZ, :NZ], hi)
-        assert np.array_equal(tiles[t + 1, :NZ, :NZ], lo)
-        for q in (t, t + 1):
-            assert not tiles[q, NZ:, :].any() and not tiles[q, :, NZ:].any()
-        assert np.max(np.abs(hi + lo - v)) <= 2.0 ** -21 * np.max(np.abs(v))
+    Qt = table(chylib, g, "Qt", NZ * NZ).reshape(NZ, NZ)   # Qt[p][k] = Q(k, p)
+    d = table(chylib, g, "dsc", NZ)
+    U = table(chylib, g, "U", NZ * NZ).reshape(NZ, NZ)
+    V = table(chylib, g, "V", NZ * NZ).reshape(NZ, NZ)
+    assert np.abs(Qt @ Qt.T - np.eye(NZ)).max() < 1e-13
+    assert np.array_equal(U, Qt * d[None, :])
+    assert np.array_equal(V, Qt.T / d[:, None])
+    z = table(chylib, g, "row_scales", 512).reshape(4, 128)
+    an, cn = table(chylib, g, "an", NZ), table(chylib, g, "cn", NZ)
+    assert np.array_equal(z[0, :NZ], d) and np.array_equal(z[1, :NZ], 1.0 / d)
+    assert np.all(z[0, NZ:] == 1.0) and np.all(z[1, NZ:] == 1.0)
+    assert z[2, 0] == 0.0 and np.array_equal(z[2, 1:NZ], d[1:] * an[1:] / d[:-1])
+    assert z[3, NZ - 1] == 0.0 and np.array_equal(z[3, :NZ - 1], d[:-1] * cn[:-1] / d[1:])
+    assert np.all(z[2:, NZ:] == 0.0)
+
+
+@pytest.mark.parametrize("J,K,L", [(64, 32, 64), (128, 128, 64)])
+def test_mixed_operand_tiles_are_hi_lo_splits(chylib, J, K, L):
+    """The eigenbasis operand of the tensor-core products, read back through
+    its K-major 128-byte-swizzled layout: hi = fp16(2^12 Q(k,p)) and
+    lo = fp16(2^12 Q(k,p) - hi) with rows p and K index k (the tile of Q^T;
+    the kernels read its transpose through the MN-major descriptor), zero
+    outside NZ x NZ; hi + lo carries 2^12 Q to about 22 bits."""
+    g = chylib.grid(J, K, L)
+    NZ = K - 1
+    tiles = table(chylib, g, "umma_tiles", 2 * 128 * 128).reshape(2, 128, 128)
+    Qt = table(chylib, g, "Qt", NZ * NZ).reshape(NZ, NZ)   # Qt[p][k]
+    v = 4096.0 * Qt
+    hi = v.astype(np.float16).astype(np.float64)
+    lo = (v - hi).astype(np.float16).astype(np.float64)
+    assert np.array_equal(tiles[0, :NZ, :NZ], hi)
+    assert np.array_equal(tiles[1, :NZ, :NZ], lo)
+    for q in (0, 1):
+        assert not tiles[q, NZ:, :].any() and not tiles[q, :, NZ:].any()
+    assert np.max(np.abs(hi + lo - v)) <= 2.0 ** -21 * np.max(np.abs(v))
 
 
 def test_boundary_splits_are_sorted_ring_counts(chylib):
@@ -215,7 +236,7 @@ def test_external_and_source_argument_checks(chylib):
     assert C.sizeof(chylib.ChyBinary) == 2 * 8
     b = chylib.ChyBinary(1.0, 100.0)
     assert L.chy_plan_set_binary(None, C.byref(b)) == 10
-    assert C.sizeof(chylib.ChyTune) == 5 * 4 + 4 + 2 * 8 + 8
+    assert C.sizeof(chylib.ChyTune) == 6 * 4 + 2 * 8 + 8
     t = chylib.ChyTune()
     assert L.chy_autotune_multi(0, None, None, None, None, 1, C.byref(t)) == 10
     assert L.chy_plan_set_schedule(None, C.byref(t)) == 10
