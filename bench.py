@@ -162,10 +162,10 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic_per_solve():
+def profiled_traffic_per_solve(kernel: str = "k_mode_pair"):
     """DRAM bytes (read + write) per solve of the mode-solve kernel from the
     committed ncu summary of that kernel, or None."""
-    path = os.path.join(HERE, "profiles", "k_mode_mixed_256x128x256.md")
+    path = os.path.join(HERE, "profiles", f"{kernel}_256x128x256.md")
     try:
         m = re.search(r"dram_bytes_per_solve:\s*([0-9]+)", open(path).read())
     except OSError:
@@ -661,9 +661,11 @@ def main():
     alg = mode_solve_bytes_per_solve() * B
     hbm, peak_kind = peaks()
     achieved = alg / (mode_ms * 1e-3) / 1e9
-    tps = profiled_traffic_per_solve() if args.precision == "mixed" else None
+    mk = chy.lib().chy_dbg_mixed_kernel(plan._p)
+    tps = profiled_traffic_per_solve({1: "k_mode_mixed", 2: "k_mode_pair"}.get(mk, "none")) \
+        if args.precision == "mixed" and (J, K, L) == (256, 128, 256) else None
     mixed_kernel = {1: "k_mode_mixed", 2: "k_mode_pair (CTA pairs, two modes per SM)",
-                    3: "wide mixed pipeline (k_wide_*)"}.get(chy.lib().chy_dbg_mixed_kernel(plan._p), "mixed")
+                    3: "wide mixed pipeline (k_wide_*)"}.get(mk, "mixed")
     kname = {"mixed": mixed_kernel,
              "fp64": "FP64 mode solves (k_zfwd_f64, k_thomas_f64, k_zinv_f64)",
              "blktri": "BLKTRI-order mode solves (k_blk_gather, k_blk_solve, k_blk_scatter)"}[args.precision]
