@@ -839,9 +839,9 @@ extern "C" int chy_plan_set_schedule(chy_plan *p, const chy_tune *c)
 {
     if (!p || !c) return fail(CHY_ERR_ARG, "null plan or schedule");
     if (c->streams < 0 || c->streams > kMultiStreams || c->chunk < 0 || c->mode_ctas < 0 ||
-        !blk_schedule_valid(c->blk_warps, c->blk_ctas_per_sm) || c->mode_kernel < 0 || c->mode_kernel > 1)
+        !blk_schedule_valid(c->blk_warps, c->blk_ctas_per_sm) || c->mode_kernel < 0 || c->mode_kernel > 2)
         return fail(CHY_ERR_ARG, "schedule out of range (streams 0..8, blk_warps 4/8/16, blk_warps * "
-                                 "blk_ctas_per_sm <= 16, mode_kernel 0/1)");
+                                 "blk_ctas_per_sm <= 16, mode_kernel 0..2)");
     p->streams = c->streams;
     p->chunk = c->chunk;
     p->mode_ctas = c->mode_ctas;
@@ -946,7 +946,7 @@ extern "C" int chy_autotune_multi(int n, chy_plan *const *plans, const double *c
         out->mode_ctas = std::max(1, uniq[0]->num_sms / best.mode_div);
         out->blk_warps = best.blk_warps;
         out->blk_ctas_per_sm = best.blk_cps;
-        out->mode_kernel = uniq[0]->mode_kernel;   // kept: it changes the result's rounding
+        out->mode_kernel = uniq[0]->mode_kernel;   // kept as set
         out->ms = best_ms;
         out->ms_default = default_ms;
         out->candidates = tried;

@@ -374,6 +374,14 @@ __device__ __forceinline__ float pow2_scale(float vmax)
     frexpf(vmax, &e);
     return ldexpf(1.0f, 14 - e);
 }
+// its exponent k: pow2_scale(vmax) = 2^k
+__device__ __forceinline__ int pow2_exp(float vmax)
+{
+    if (!(vmax > 0.0f) || !isfinite(vmax)) return 0;
+    int e;
+    frexpf(vmax, &e);
+    return 14 - e;
+}
 
 // Writes the FP16 hi/lo split of v (already scaled) for element (row, k).
 __device__ __forceinline__ void put_split(uint8_t *hi, uint8_t *lo, int row, int k, int R, float v)
@@ -480,8 +488,8 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
     double *d_an = d_bm + 256, *d_bn = d_an + 128, *d_cn = d_bn + 128;         // [128] each
     float4 *f_t = reinterpret_cast<float4 *>(d_cn + 128);                     // [256] {g, a, c, 0}
     float *f_lam = reinterpret_cast<float *>(f_t + 256);                       // [128]
-    float *f_red = f_lam + 128;                                                // [8]
-    double *d_red = reinterpret_cast<double *>(f_red + 8);                     // [24]
+    float *f_red = f_lam + 128;                                                // [2][8]
+    double *d_red = reinterpret_cast<double *>(f_red + 16);                    // [24]
     float *f_xch = reinterpret_cast<float *>(d_red + 24);                      // [128][4]
     float *f_edge = f_xch + 512;                                               // [2][8][2][16]
     uint64_t *bar_mma = reinterpret_cast<uint64_t *>(f_edge + 512);
@@ -605,7 +613,12 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
         double *Xl = w.X + (size_t)b * w.sX + (size_t)l * K * J;
         double *xl = kRes ? nullptr : x.xbuf + (size_t)b * x.sxb + (size_t)l * K * J;
         double *cr = x.corr + (size_t)b * x.scorr + (size_t)l * 16;
-        double u0 = 0.0;   // kRes: scale of x0 held in tensor memory
+        // kRes: scales 2^eu0 of x0 held in tensor memory, per radial half
+        // [0, NT/2) and [NT/2, NT): every power-of-two scale is taken per half,
+        // exactly as k_mode_pair's two CTAs take them, so both kernels give the
+        // same bits
+        double u0h0 = 0.0, u0h1 = 0.0;
+        int eu0h0 = 0, eu0h1 = 0;
         double ym_keep = 0.0;   // kRes: X(k, M) of this thread's row, for the write-back tiles
         __syncthreads();
 
@@ -613,13 +626,13 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             const bool last = it == nit - 1;
             const bool res_x = kRes && it > 0;          // x0 read from tensor memory
             const uint32_t acc = res_x ? 256u : 0u;     // product / sweep columns
-            float sxf = 0.f;                            // kRes: sum of x0^2 (unscaled)
+            float sxf0 = 0.f, sxf1 = 0.f;               // kRes: sums of x0^2 per half (unscaled)
             // ---- residual r = Y - A_m x (FP64) -> TMEM cols [256, 256+NT) as FP32.
             // Out-of-range neighbours read as 0; their stencil coefficients
             // (AN(1), CN(KMAX-1), AM(1), CM(JMAX-1)) are 0 too.  JMAX is a
             // multiple of 16, so column M is in the chunk of column M-1 and
             // every 16-byte granule of a row is aligned.
-            float rmax = 0.0f;
+            float rmax0 = 0.0f, rmax1 = 0.0f;           // max |r| per half
             if constexpr (kRes) {
                 // Raw X rows k = 0..KMAX-1 (boundary row NZ and column M
                 // included) stream through a four-deep ring of 32-column
@@ -745,11 +758,16 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                         const float *ed = f_edge + ((c & 1) * 8 + (quad < 3 ? warp + 1 : warp)) * 32;
                         const bool top0 = lane == 0, bot31 = lane == 31;
                         const float zu = quad > 0 ? 1.f : 0.f, zd = quad < 3 ? 1.f : 0.f;
-                        double xd_[18];   // x0 at columns j-1 .. j+16 (unscaled)
-                        xd_[0] = (double)xlf;
-                        xd_[17] = (double)xrt;
+                        // x0 at columns j-1 .. j+16 in this half's units; a neighbour
+                        // across the halves' boundary is converted exactly
+                        const bool hh = c0 >= NH;
+                        const double u0 = hh ? u0h1 : u0h0;
+                        double xd_[18];
+                        xd_[0] = c0 + jb == NH ? ldexp((double)xlf, eu0h0 - eu0h1) : (double)xlf;
+                        xd_[17] = c0 + jb + 16 == NH ? ldexp((double)xrt, eu0h1 - eu0h0) : (double)xrt;
 #pragma unroll
                         for (int u = 0; u < 16; ++u) xd_[u + 1] = (double)xc[u];
+                        float sxf = 0.f, rm = 0.f;
 #pragma unroll
                         for (int u = 0; u < 16; ++u) {
                             const int j = c0 + jb + u;
@@ -769,15 +787,20 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                             const bool in = krow && j < M;
                             sxf = fmaf(in ? xc[u] : 0.f, xc[u], sxf);
                             v[u] = in ? (float)r : 0.f;
-                            rmax = fmaxf(rmax, fabsf(v[u]));
+                            rm = fmaxf(rm, fabsf(v[u]));
                         }
+                        if (hh) { rmax1 = fmaxf(rmax1, rm); sxf1 += sxf; }
+                        else { rmax0 = fmaxf(rmax0, rm); sxf0 += sxf; }
                     } else {
+                        float rm = 0.f;
 #pragma unroll
                         for (int u = 0; u < 16; ++u) {
                             const int j = c0 + jb + u;
                             v[u] = (krow && j < M) ? (float)yv[u] : 0.f;
-                            rmax = fmaxf(rmax, fabsf(v[u]));
+                            rm = fmaxf(rm, fabsf(v[u]));
                         }
+                        if (c0 >= NH) rmax1 = fmaxf(rmax1, rm);
+                        else rmax0 = fmaxf(rmax0, rm);
                     }
                     tm_st16_nw(tmem + lane_base + 256 + c0 + jb, v);
                 }
@@ -863,21 +886,25 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                             }
                         }
                         v[u] = (float)(dk * r);
-                        rmax = fmaxf(rmax, fabsf(v[u]));
+                        if (c0 >= NH) rmax1 = fmaxf(rmax1, fabsf(v[u]));
+                        else rmax0 = fmaxf(rmax0, fabsf(v[u]));
                     }
                     tm_st8(tmem + lane_base + 256 + c0 + jb, v);
                     __syncthreads();
                 }
                 tm_wait_st();
             }
-            rmax = warp_max(rmax);
-            if (lane == 0) f_red[warp] = rmax;
+            rmax0 = warp_max(rmax0);
+            rmax1 = warp_max(rmax1);
+            if (lane == 0) { f_red[warp] = rmax0; f_red[8 + warp] = rmax1; }
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
-            rmax = f_red[0];
-            for (int i = 1; i < 8; ++i) rmax = fmaxf(rmax, f_red[i]);
-            const float s1 = pow2_scale(rmax);
+            rmax0 = f_red[0];
+            rmax1 = f_red[8];
+            for (int i = 1; i < 8; ++i) { rmax0 = fmaxf(rmax0, f_red[i]); rmax1 = fmaxf(rmax1, f_red[8 + i]); }
+            const int k1h0 = pow2_exp(rmax0), k1h1 = pow2_exp(rmax1);
+            const float s1 = ldexpf(1.0f, jh ? k1h1 : k1h0);   // this thread splits half jh
             // ---- TMEM r -> B tile (row j, K index k), FP16 hi/lo
             for (int c0 = jh * NH; c0 < (jh + 1) * NH; c0 += 32) {
                 float v[32];
@@ -973,14 +1000,19 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 const bool cv_ok = wait_all(bar_cv, ph_cv);
                 if (!cv_ok) { failed = true; break; }
                 cv_pend = false;
-                // meeting rows h-1 (top) and h (bottom):
+                // meeting rows h-1 (top) and h (bottom), in FP64 from the two
+                // halves' values at their own scales 2^(12 + k1):
                 // x_t = y'_t + (1-e_t) x_u, x_u = y''_u + (1-f_u) x_t
                 float xt, xu;
                 {
-                    const float yt = f_xch[p * 4 + 0], et = cvs[(h - 1) * 128 + p];
-                    const float yu = f_xch[p * 4 + 2], fu = cvs[h * 128 + p];
-                    xt = (yt + (1.0f - et) * yu) / ((et + fu) - et * fu);
-                    xu = yu + (1.0f - fu) * xt;
+                    const int ks0 = 12 + k1h0, ks1 = 12 + k1h1;
+                    const double yt = ldexp((double)f_xch[p * 4 + 0], -ks0);
+                    const double yu = ldexp((double)f_xch[p * 4 + 2], -ks1);
+                    const double et = cvs[(h - 1) * 128 + p], fu = cvs[h * 128 + p];
+                    const double xtd = (yt + (1.0 - et) * yu) / ((et + fu) - et * fu);
+                    const double xud = yu + (1.0 - fu) * xtd;
+                    xt = (float)ldexp(xtd, ks0);
+                    xu = (float)ldexp(xud, ks1);
                 }
                 if (jh == 0) {
                     float xn = xt;   // x_{j+1} while sweeping up
@@ -1017,14 +1049,16 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 }
                 tm_wait_st();
             }
+            // per half: warps 0-3 swept half 0, warps 4-7 half 1
             xmax = warp_max(xmax);
             if (lane == 0) f_red[warp] = xmax;
             tc_fence_before();
             __syncthreads();
             tc_fence_after();
-            xmax = f_red[0];
-            for (int i = 1; i < 8; ++i) xmax = fmaxf(xmax, f_red[i]);
-            const float s2 = pow2_scale(xmax);
+            float xm0 = f_red[0], xm1 = f_red[4];
+            for (int i = 1; i < 4; ++i) { xm0 = fmaxf(xm0, f_red[i]); xm1 = fmaxf(xm1, f_red[4 + i]); }
+            const int k2h0 = pow2_exp(xm0), k2h1 = pow2_exp(xm1);
+            const float s2 = ldexpf(1.0f, jh ? k2h1 : k2h0);
             // ---- TMEM w -> B tile (row j, K index p), FP16 hi/lo
             for (int c0 = jh * NH; c0 < (jh + 1) * NH; c0 += 32) {
                 float v[32];
@@ -1043,10 +1077,16 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             if (!wait_all(bar_mma, ph_mma)) { failed = true; break; }
             mma_pend = false;
             tc_fence_after();
-            const double unscale = 1.0 / ((double)kAScale * (double)kAScale * (double)s1 * (double)s2);
+            // this solve's columns are 2^eun times its result, per half
+            const int eun0 = -(24 + k1h0 + k2h0), eun1 = -(24 + k1h1 + k2h1);
+            const double unscale0 = ldexp(1.0, eun0), unscale1 = ldexp(1.0, eun1);
             if constexpr (kRes) {
                 if (!last) {
-                    u0 = unscale;   // x0 stays in tensor memory columns [0, NT)
+                    // x0 stays in tensor memory columns [0, NT)
+                    u0h0 = unscale0;
+                    u0h1 = unscale1;
+                    eu0h0 = eun0;
+                    eu0h1 = eun1;
                     continue;
                 }
                 // X = x0 + delta (FP64).  Each 32-column chunk is staged in
@@ -1057,13 +1097,14 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 // tensor-memory rows load while this chunk's tiles are stored.
                 double sd = 0.0, sx = 0.0;
                 const int jb = jh * 16, row0 = (b * t.L + l) * K;
-                const double uk = unscale * ek, u0k = u0 * ek;   // this row's 1/d_k
                 float dv[16], xv[16];
                 tm_ld16_nw(tmem + lane_base + acc + jb, dv);
                 if (res_x) tm_ld16_nw(tmem + lane_base + jb, xv);
                 for (int c0 = 0, c = 0; c0 < NT; c0 += 32, ++c) {
                     uint8_t *slot = sBh + (c % 3) * kRingSlot;
                     tm_wait_ld32(dv, xv);
+                    const bool hh = c0 >= NH;
+                    const double uk = (hh ? unscale1 : unscale0) * ek, u0k = (hh ? u0h1 : u0h0) * ek;   // row's 1/d_k
                     double xn[16];
 #pragma unroll
                     for (int u = 0; u < 16; ++u) {
@@ -1097,11 +1138,11 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                 }
                 if (tid == 0) bulk_wait_all();   // tiles written, staging free for the next item
                 __syncthreads();
-                block_sum3(sd, sx, (double)sxf * ek * ek);
+                block_sum3(sd, sx, ((double)sxf0 * u0h0 * u0h0 + (double)sxf1 * u0h1 * u0h1) * ek * ek);
                 if (tid == 0) {
                     if (res_x) {   // the first solve's delta is x0 itself
-                        cr[0] = d_red[16] * u0 * u0;
-                        cr[1] = d_red[16] * u0 * u0;
+                        cr[0] = d_red[16];
+                        cr[1] = d_red[16];
                     }
                     cr[2 * it] = d_red[0];
                     cr[2 * it + 1] = d_red[8];
@@ -1139,7 +1180,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
                     float v[16];
                     tm_ld16(tmem + lane_base + c0 + jb, v);
 #pragma unroll
-                    for (int u = 0; u < 16; ++u) sD[kq * 33 + jb + u] = (double)v[u] * (unscale * ek);
+                    for (int u = 0; u < 16; ++u) sD[kq * 33 + jb + u] = (double)v[u] * ((c0 >= NH ? unscale1 : unscale0) * ek);
                     __syncthreads();
                     const double *so = sO + (c & 1) * (128 * 32);
                     for (int i = tid; i < 128 * 32; i += 256) {
@@ -1289,14 +1330,6 @@ __device__ __forceinline__ bool mbar_wait_cl(uint64_t *bar, uint32_t parity)
 __device__ __forceinline__ void cluster_sync_all()
 {
     asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-// power-of-two exponent k of pow2_scale(vmax) = 2^k
-__device__ __forceinline__ int pow2_exp(float vmax)
-{
-    if (!(vmax > 0.0f) || !isfinite(vmax)) return 0;
-    int e;
-    frexpf(vmax, &e);
-    return 14 - e;
 }
 
 __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, MixedDev x, int nb,
@@ -2391,8 +2424,10 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
     if (d.nit <= 2 && !p->mx->tm_ok) return CHY_ERR_CUDA;   // tensor map over X not encoded
     const long long items = (long long)nb * p->hp.L;
     const int cap = p->mode_ctas > 0 && p->mode_ctas < p->num_sms ? p->mode_ctas : p->num_sms;
-    if (d.nit <= 2 && p->mode_kernel == 0) {
-        // CTA pairs, two items per CTA
+    if (d.nit <= 2 && p->mode_kernel != 1) {
+        // CTA pairs, two items per CTA: chosen (mode_kernel 0) when each group
+        // gets at least 16 items, so that the second group's half-item start
+        // delay is paid back; both kernels give the same bits
         MixedState &ms = *p->mx;
         if (ms.pair_clusters < 0) {
             ms.pair_clusters = 0;
@@ -2413,7 +2448,7 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
                 cudaGetLastError();
             }
         }
-        if (ms.pair_clusters > 0) {
+        if (ms.pair_clusters > 0 && (p->mode_kernel == 2 || items >= 32ll * ms.pair_clusters)) {
             long long pairs = (items + 1) / 2;
             pairs = std::min<long long>(pairs, ms.pair_clusters);
             pairs = std::min<long long>(pairs, std::max(1, cap / 2));

@@ -24,7 +24,7 @@ struct chy_plan {
     int device = 0;                // the device the plan's tables and work space live on
     // launch schedule (chy_autotune_multi picks these; 0 = the default)
     int mode_ctas = 0;             // persistent CTAs of the fused mixed mode solve (default: one per SM)
-    int mode_kernel = 0;           // fused mixed mode solve: 0 CTA pairs (k_mode_pair), 1 one CTA per item
+    int mode_kernel = 0;           // fused mixed mode solve: 0 auto, 1 one CTA per item, 2 CTA pairs (k_mode_pair)
     int blk_warps = 8;             // BLKTRI order: warps per CTA (4, 8, 16)
     int blk_ctas_per_sm = 2;       // BLKTRI order: CTAs per SM (blk_warps * this <= 16)
     int chunk = 0;                 // chy_solve_multi: solves per launch sequence (default max_batch)

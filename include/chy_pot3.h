@@ -145,10 +145,11 @@ int chy_solve_multi(int n, chy_plan *const *plans, const double *const *rho, dou
  *   chunk        solves per launch sequence (max_batch, /2, /4);
  *   mode_ctas    persistent CTAs of each fused mixed mode solve (all SMs, 1/2,
  *                1/4: grids running side by side then share the SMs);
- *   mode_kernel  not searched (the two kernels round the mixed result
- *                differently, within the same tolerance): the plan's own
- *                setting, 0 = CTA pairs holding two (solve, mode) items per
- *                SM (default), 1 = one CTA per item;
+ *   mode_kernel  not searched; the plan's own setting for the fused mixed
+ *                mode solve: 0 = automatic (CTA pairs when the launch holds
+ *                at least 16 (solve, mode) items per group of warps, else
+ *                one CTA per item), 1 = one CTA per item, 2 = CTA pairs
+ *                holding two items per SM.  Both kernels give the same bits;
  *   blk_warps,   the BLKTRI-order path's stage schedule: warps per CTA (the
  *   blk_ctas_per_sm  cyclic-reduction tasks of a stage in flight at once) and
  *                CTAs per SM.

@@ -79,27 +79,46 @@ def test_mixed_meets_1e10(chylib, cfg):
 
 @pytest.mark.parametrize("J,K,L", [(256, 128, 64), (64, 32, 64), (80, 32, 64), (192, 64, 32)])
 def test_mixed_mode_kernels(chylib, J, K, L):
-    """Both fused mode-solve kernels meet 1e-10 against the oracle: the
-    default k_mode_pair (a CTA pair per mode, two modes per SM, the sweeps'
-    meeting rows and the iterate's edge column exchanged through distributed
-    shared memory) and k_mode_mixed (one CTA per mode, mode_kernel = 1).
-    Each is deterministic: a mode's result does not depend on the batch
-    around it or on which CTAs solved it."""
+    """The two fused mode-solve kernels -- k_mode_pair (a CTA pair per mode,
+    two modes per SM, the sweeps' meeting rows and the iterate's edge column
+    exchanged through distributed shared memory) and k_mode_mixed (one CTA
+    per mode) -- take every power-of-two scale per radial half and give the
+    same bits; both meet 1e-10 against the oracle.  A mode's result does not
+    depend on the batch around it or on which CTAs solved it."""
     rho, ref, _, _ = oracle_result((J, K, L), seed_override=17)
     rho2 = synth.disk_density(J, K, L, 18, spiral=True, spectrum=True)
     ws = write_set(J, K)
     outs = {}
-    for mk, kernel in ((0, 2), (1, 1)):
+    for mk, kernel in ((2, 2), (1, 1), (0, 1)):
         plan = chylib.Plan(chylib.grid(J, K, L), "mixed", 3)
         plan.set_schedule(mode_kernel=mk)
         (single,), (d,) = plan.solve_batch([rho], diag=True)
+        # mode_kernel 0 (automatic) keeps one CTA per mode for so few modes
         assert chylib.lib().chy_dbg_mixed_kernel(plan._p) == kernel
         assert rel_l2(single[ws], ref[ws]) < 1e-10
         assert d["iterations"] == 2 and d["corr_rel"][0] == pytest.approx(1.0) and d["corr_rel"][1] < 1e-5
         batch = plan.solve_batch([rho, rho2, rho])
         assert np.array_equal(batch[0], single) and np.array_equal(batch[2], single)
         outs[mk] = single
-    assert rel_l2(outs[0][ws], outs[1][ws]) < 1e-10
+    assert np.array_equal(outs[2], outs[1]) and np.array_equal(outs[0], outs[1])
+
+
+def test_mixed_automatic_kernel_choice(chylib):
+    """mode_kernel 0 runs k_mode_pair once the launch holds at least 16 modes
+    per group of warps (32 per CTA pair) and one CTA per mode below that;
+    the results are the same bits either way."""
+    import torch
+    J, K, L = 64, 32, 256
+    g = chylib.grid(J, K, L)
+    rhos = [chylib.to_cuda_fortran(synth.disk_density(J, K, L, 40 + i, spiral=True, spectrum=True)) for i in range(20)]
+    plan = chylib.Plan(g, "mixed", 20)
+    small = plan.solve_batch(rhos[:1])
+    torch.cuda.synchronize()
+    assert chylib.lib().chy_dbg_mixed_kernel(plan._p) == 1
+    big = plan.solve_batch(rhos)              # 20 x 256 modes >= 32 x 74 pairs
+    torch.cuda.synchronize()
+    assert chylib.lib().chy_dbg_mixed_kernel(plan._p) == 2
+    assert torch.equal(small[0], big[0])
 
 
 def test_mixed_refinement_converges_geometrically(chylib):
