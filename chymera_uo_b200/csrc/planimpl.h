@@ -63,17 +63,22 @@ struct chy_plan {
     MixedState *mx = nullptr;
 };
 
-// Copies the write set of one solve's PHI from device to the caller's host
-// array: PHI(1:JMAX+1, 1, :) and PHI(:, 2:KMAX+1, :).  PHI(:, KMAX+2, :) and
-// PHI(JMAX+2, 1, :) are never written by a solve, so the host keeps its own
-// values there and the device copy never needs them.
-inline cudaError_t copy_phi_write_set(double *host, const double *dev, int J, int K, int L, cudaStream_t s)
+// Host <-> device copies of host-pointer solves are single linear copies:
+// with copies running in both directions at once, pitched (2-D) copies of the
+// same rows reached about 12% less PCIe throughput on B200 hosts.
+//
+// Copies one solve's PHI from device to the caller's host array as one span,
+// PHI(1,1,1) .. PHI(JMAX+2, KMAX+1, LMAX): the write set (PHI(1:JMAX+1, 1, :)
+// and PHI(:, 2:KMAX+1, :)) and, between its pieces, the cells a solve never
+// writes (PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :), all but the last plane's
+// row KMAX+2).  Those cells of the device copy hold the caller's own values,
+// copied in by copy_phi_rim earlier in the same call, so the host gets them
+// back unchanged.
+inline cudaError_t copy_phi_out(double *host, const double *dev, int J, int K, int L, cudaStream_t s)
 {
-    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2, plane = J2 * K2 * sizeof(double);
-    cudaError_t e = cudaMemcpy2DAsync(host + J2, plane, dev + J2, plane, (size_t)K * J2 * sizeof(double), L,
-                                      cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) return e;
-    return cudaMemcpy2DAsync(host, plane, dev, plane, ((size_t)J + 1) * sizeof(double), L, cudaMemcpyDeviceToHost, s);
+    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2;
+    const size_t n = (size_t)(L - 1) * J2 * K2 + ((size_t)K + 1) * J2;
+    return cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, s);
 }
 
 // Copies the rows of RHO a solve reads, RHO(:, 2:nrows+1, :), from the
@@ -83,9 +88,11 @@ inline cudaError_t copy_phi_write_set(double *host, const double *dev, int J, in
 inline cudaError_t copy_rho_read_set(double *dev, const double *host, int J, int K, int L, int nrows,
                                      cudaStream_t s)
 {
-    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2, plane = J2 * K2 * sizeof(double);
-    return cudaMemcpy2DAsync(dev + J2, plane, host + J2, plane, (size_t)nrows * J2 * sizeof(double), L,
-                             cudaMemcpyHostToDevice, s);
+    // one span from row 2 of the first plane to row nrows+1 of the last: the
+    // rows in between planes come along, and no solve reads them
+    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2;
+    const size_t n = (size_t)(L - 1) * J2 * K2 + (size_t)nrows * J2;
+    return cudaMemcpyAsync(dev + J2, host + J2, n * sizeof(double), cudaMemcpyHostToDevice, s);
 }
 
 // Copies the cells of PHI that a solve never writes, PHI(:, KMAX+2, :) and

@@ -250,6 +250,9 @@ int chy_server::launch(SizeClass &c, Lane &ln)
         Request *rq = ln.batch[i];
         double *dr = reinterpret_cast<double *>(arena_base + rq->buf_off), *df = dr + c.nvol;
         if (copy_rho_read_set(dr, rq->rho, c.J, c.K, c.L, c.K - 1, ln.stream) != cudaSuccess) return CHY_ERR_CUDA;
+        // the cells the solve leaves alone go back with the rest of PHI
+        if (copy_phi_rim(df, rq->phi, c.J, c.K, c.L, cudaMemcpyHostToDevice, ln.stream) != cudaSuccess)
+            return CHY_ERR_CUDA;
         bp.rho[i] = dr;
         bp.phi[i] = df;
     }
@@ -262,7 +265,7 @@ int chy_server::launch(SizeClass &c, Lane &ln)
         if (st != CHY_OK) return st;
     }
     for (int i = 0; i < nb; i++)
-        if (copy_phi_write_set(ln.batch[i]->phi, bp.phi[i], c.J, c.K, c.L, ln.stream) != cudaSuccess)
+        if (copy_phi_out(ln.batch[i]->phi, bp.phi[i], c.J, c.K, c.L, ln.stream) != cudaSuccess)
             return CHY_ERR_CUDA;
     if (cudaEventRecord(ln.done, ln.stream) != cudaSuccess) return CHY_ERR_CUDA;
     return CHY_OK;

@@ -113,7 +113,11 @@ void chy_plan_destroy(chy_plan *p);
 
 /* One solve: BDYGEN(MAXTRM,ISYM,REDGE) then POT3(NPOINT,IPRINT=0).
  * rho/phi are device pointers (CHY_PTR_DEVICE) or host pointers
- * (CHY_PTR_HOST; pinned memory gives full copy bandwidth).  stream may be
+ * (CHY_PTR_HOST; pinned memory gives full copy bandwidth).  A device PHI
+ * changes in the reference's write set only.  A host PHI comes back as one
+ * contiguous copy: the cells outside the write set (PHI(:,KMAX+2,:),
+ * PHI(JMAX+2,1,:)) are read at the start of the call and written back with
+ * the same values.  stream may be
  * NULL (legacy default stream).  diag may be NULL.  For device pointers the
  * call is asynchronous unless diag is non-NULL.  Device RHO arrays that start
  * on a 16-byte boundary (cudaMalloc and torch allocations do) with JMAX even
@@ -196,8 +200,10 @@ typedef struct chy_server_stats {
 /* Starts the dispatcher on the current device; allocates the arena. */
 int chy_server_create(const chy_server_opts *o, chy_server **out);
 /* Queues one solve of grid g (arrays copied now): rho is read and phi written
- * (the reference's write set) asynchronously; both must stay valid until
- * chy_server_wait returns.  Pinned host memory gives full copy bandwidth. */
+ * (the reference's write set; the cells outside it are read and written back
+ * unchanged, as for CHY_PTR_HOST solves) asynchronously; both must stay valid
+ * until chy_server_wait returns.  Pinned host memory gives full copy
+ * bandwidth. */
 int chy_server_submit(chy_server *s, const chy_grid *g, const double *rho, double *phi, long long *ticket);
 /* Blocks until the request is done; returns its status and the latency from
  * submission to completion (host clock, ms). */
