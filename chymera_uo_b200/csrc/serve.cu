@@ -4,8 +4,9 @@
 // chy_server_submit from any thread.  One dispatcher thread:
 //   * keeps one size class per distinct grid: plans (tables + work space) that
 //     stay resident on the device and are reused by every later request of
-//     that grid, two "lanes" per class so that the copies of one batch overlap
-//     the solves of the previous one;
+//     that grid, two "lanes" per class, each with up to two batches in flight
+//     on three streams (copies in, solves, copies out), so that a batch's
+//     copies overlap the solves and copies of the others;
 //   * admits waiting requests into a free lane as soon as device buffers for
 //     them fit in the arena (the HBM budget left after the plans), up to the
 //     plan's batch size -- requests that arrive while others are on the GPU
@@ -40,6 +41,7 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 constexpr int kLanes = 2;
+constexpr int kLaneDepth = 2;   // batches in flight per lane
 
 struct Request {
     long long id = 0;
@@ -55,12 +57,55 @@ struct Request {
     size_t buf_off = 0;                   // device buffers [rho | phi] in the arena
 };
 
+// One batch in flight: its requests, the events that order its copies in,
+// solve and copies out, and the pinned word its mode solve's error word is
+// read back into.
+struct Slot {
+    std::vector<Request *> batch;
+    cudaEvent_t in = nullptr, solved = nullptr, done = nullptr;
+    int *err = nullptr;
+};
+
 struct Lane {
     chy_plan *plan = nullptr;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t done = nullptr;
-    std::vector<Request *> batch;
+    cudaStream_t stream = nullptr;                 // solves (in order: they share the plan's work space)
+    cudaStream_t s_in = nullptr, s_out = nullptr;  // host -> device, device -> host copies
+    Slot slots[kLaneDepth];
+    bool idle() const
+    {
+        for (const Slot &sl : slots)
+            if (!sl.batch.empty()) return false;
+        return true;
+    }
 };
+
+int lane_streams(Lane &ln)
+{
+    if (cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ln.s_in, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ln.s_out, cudaStreamNonBlocking) != cudaSuccess)
+        return CHY_ERR_CUDA;
+    for (Slot &sl : ln.slots)
+        if (cudaEventCreateWithFlags(&sl.in, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.solved, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost(&sl.err, sizeof(int)) != cudaSuccess)
+            return CHY_ERR_CUDA;
+    return CHY_OK;
+}
+
+void lane_free(Lane &ln)
+{
+    if (ln.plan) chy_plan_destroy(ln.plan);
+    for (cudaStream_t st : {ln.stream, ln.s_in, ln.s_out})
+        if (st) cudaStreamDestroy(st);
+    for (Slot &sl : ln.slots) {
+        for (cudaEvent_t ev : {sl.in, sl.solved, sl.done})
+            if (ev) cudaEventDestroy(ev);
+        if (sl.err) cudaFreeHost(sl.err);
+    }
+    ln = Lane{};
+}
 
 struct SizeClass {
     std::string key;
@@ -164,8 +209,8 @@ struct chy_server {
     std::thread worker;
 
     void run();
-    int launch(SizeClass &c, Lane &ln);
-    void retire(SizeClass &c, Lane &ln, int status);
+    int launch(SizeClass &c, Lane &ln, Slot &sl);
+    void retire(SizeClass &c, Slot &sl, int status);
     int make_class(Request *rq, SizeClass **out);
 };
 
@@ -191,21 +236,17 @@ int chy_server::make_class(Request *rq, SizeClass **out)
             prec = CHY_PREC_FP64;
             st = chy_plan_create(&g, prec, max_batch, &ln.plan);
         }
+        if (st == CHY_OK) {
+            plan_bytes += (size_t)chy_plan_device_bytes(ln.plan);
+            st = lane_streams(ln);
+        }
         if (st != CHY_OK) {
             for (int k = 0; k <= i; k++) {
-                if (c->lanes[k].plan) {
-                    plan_bytes -= (size_t)chy_plan_device_bytes(c->lanes[k].plan);
-                    chy_plan_destroy(c->lanes[k].plan);
-                }
-                if (c->lanes[k].stream) cudaStreamDestroy(c->lanes[k].stream);
-                if (c->lanes[k].done) cudaEventDestroy(c->lanes[k].done);
+                if (c->lanes[k].plan) plan_bytes -= (size_t)chy_plan_device_bytes(c->lanes[k].plan);
+                lane_free(c->lanes[k]);
             }
             return st;
         }
-        plan_bytes += (size_t)chy_plan_device_bytes(ln.plan);
-        if (cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&ln.done, cudaEventDisableTiming) != cudaSuccess)
-            return CHY_ERR_CUDA;
     }
     c->last_use = Clock::now();
     // plans count against the budget left after the arena: drop idle classes
@@ -215,24 +256,20 @@ int chy_server::make_class(Request *rq, SizeClass **out)
         for (auto &kv : classes) {
             SizeClass &o = *kv.second;
             bool idle = o.waiting.empty();
-            for (Lane &ln : o.lanes) idle = idle && ln.batch.empty();
+            for (Lane &ln : o.lanes) idle = idle && ln.idle();
             if (idle && (!victim || o.last_use < victim->last_use)) victim = &o;
         }
         if (!victim) break;
         for (Lane &ln : victim->lanes) {
             plan_bytes -= (size_t)chy_plan_device_bytes(ln.plan);
-            chy_plan_destroy(ln.plan);
-            cudaStreamDestroy(ln.stream);
-            cudaEventDestroy(ln.done);
+            lane_free(ln);
         }
         classes.erase(victim->key);
     }
     if (plan_bytes > budget - arena.size || c->req_bytes > arena.size) {
         for (Lane &ln : c->lanes) {
             plan_bytes -= (size_t)chy_plan_device_bytes(ln.plan);
-            chy_plan_destroy(ln.plan);
-            cudaStreamDestroy(ln.stream);
-            cudaEventDestroy(ln.done);
+            lane_free(ln);
         }
         return CHY_ERR_CAPACITY;
     }
@@ -241,47 +278,52 @@ int chy_server::make_class(Request *rq, SizeClass **out)
     return CHY_OK;
 }
 
-// Copies in, solves and copies out the lane's batch on its stream.
-int chy_server::launch(SizeClass &c, Lane &ln)
+// Copies the slot's batch in (s_in), solves it (the lane's solve stream, after
+// the lane's earlier batches) and copies it out (s_out).
+int chy_server::launch(SizeClass &c, Lane &ln, Slot &sl)
 {
     BatchPtrs bp{};
-    const int nb = (int)ln.batch.size();
+    const int nb = (int)sl.batch.size();
     for (int i = 0; i < nb; i++) {
-        Request *rq = ln.batch[i];
+        Request *rq = sl.batch[i];
         double *dr = reinterpret_cast<double *>(arena_base + rq->buf_off), *df = dr + c.nvol;
-        if (copy_rho_read_set(dr, rq->rho, c.J, c.K, c.L, c.K - 1, ln.stream) != cudaSuccess) return CHY_ERR_CUDA;
+        if (copy_rho_read_set(dr, rq->rho, c.J, c.K, c.L, c.K - 1, ln.s_in) != cudaSuccess) return CHY_ERR_CUDA;
         // the cells the solve leaves alone go back with the rest of PHI
-        if (copy_phi_rim(df, rq->phi, c.J, c.K, c.L, cudaMemcpyHostToDevice, ln.stream) != cudaSuccess)
+        if (copy_phi_rim(df, rq->phi, c.J, c.K, c.L, cudaMemcpyHostToDevice, ln.s_in) != cudaSuccess)
             return CHY_ERR_CUDA;
         bp.rho[i] = dr;
         bp.phi[i] = df;
     }
+    if (cudaEventRecord(sl.in, ln.s_in) != cudaSuccess || cudaStreamWaitEvent(ln.stream, sl.in, 0) != cudaSuccess)
+        return CHY_ERR_CUDA;
     int st = chy_internal_run_batch(ln.plan, bp, nb, ln.stream);
     if (st != CHY_OK) return st;
-    // the mode solve's error word, read back with the batch (checked at retirement)
-    if (int *ew = chy_mixed_host_error_word(ln.plan)) {
-        *ew = 0;
-        st = chy_mixed_read_error(ln.plan, ew, ln.stream);
-        if (st != CHY_OK) return st;
-    }
+    // the mode solve's error word, read back with the batch into the slot's own
+    // word (checked at retirement; no-op for other precisions)
+    *sl.err = 0;
+    st = chy_mixed_read_error(ln.plan, sl.err, ln.stream);
+    if (st != CHY_OK) return st;
+    if (cudaEventRecord(sl.solved, ln.stream) != cudaSuccess ||
+        cudaStreamWaitEvent(ln.s_out, sl.solved, 0) != cudaSuccess)
+        return CHY_ERR_CUDA;
     for (int i = 0; i < nb; i++)
-        if (copy_phi_out(ln.batch[i]->phi, bp.phi[i], c.J, c.K, c.L, ln.stream) != cudaSuccess)
+        if (copy_phi_out(sl.batch[i]->phi, bp.phi[i], c.J, c.K, c.L, ln.s_out) != cudaSuccess)
             return CHY_ERR_CUDA;
-    if (cudaEventRecord(ln.done, ln.stream) != cudaSuccess) return CHY_ERR_CUDA;
+    if (cudaEventRecord(sl.done, ln.s_out) != cudaSuccess) return CHY_ERR_CUDA;
     return CHY_OK;
 }
 
-void chy_server::retire(SizeClass &c, Lane &ln, int status)
+void chy_server::retire(SizeClass &c, Slot &sl, int status)
 {
     const auto now = Clock::now();
-    for (Request *rq : ln.batch) {
+    for (Request *rq : sl.batch) {
         arena.release(rq->buf_off, c.req_bytes);
         rq->status = status;
         rq->latency_ms = std::chrono::duration<double, std::milli>(now - rq->t_submit).count();
         rq->done = true;
         completed++;
     }
-    ln.batch.clear();
+    sl.batch.clear();
     c.last_use = now;
 }
 
@@ -321,36 +363,48 @@ void chy_server::run()
         // retire finished batches
         for (auto &kv : classes)
             for (Lane &ln : kv.second->lanes)
-                if (!ln.batch.empty()) {
-                    const cudaError_t e = cudaEventQuery(ln.done);
-                    if (e == cudaErrorNotReady) continue;
-                    const int *ew = chy_mixed_host_error_word(ln.plan);
-                    retire(*kv.second, ln, e != cudaSuccess ? CHY_ERR_CUDA : (ew && *ew) ? CHY_ERR_TIMEOUT : CHY_OK);
-                    progress = true;
-                }
-        // admit waiting requests into idle lanes while their buffers fit
+                for (Slot &sl : ln.slots)
+                    if (!sl.batch.empty()) {
+                        const cudaError_t e = cudaEventQuery(sl.done);
+                        if (e == cudaErrorNotReady) continue;
+                        retire(*kv.second, sl, e != cudaSuccess ? CHY_ERR_CUDA : *sl.err ? CHY_ERR_TIMEOUT : CHY_OK);
+                        progress = true;
+                    }
+        // admit waiting requests into free slots while their buffers fit: the
+        // lanes' first slots before their second ones, so that batches spread
+        // over both lanes' solve streams
         for (auto &kv : classes) {
             SizeClass &c = *kv.second;
-            for (Lane &ln : c.lanes) {
-                if (c.waiting.empty()) break;
-                if (!ln.batch.empty()) continue;
-                while (!c.waiting.empty() && (int)ln.batch.size() < max_batch) {
-                    size_t off = 0;
-                    if (!arena.alloc(c.req_bytes, &off)) break;
-                    Request *rq = c.waiting.front();
-                    c.waiting.pop_front();
-                    rq->buf_off = off;
-                    ln.batch.push_back(rq);
+            bool full = false;
+            for (int d = 0; d < kLaneDepth && !full; d++)
+                for (Lane &ln : c.lanes) {
+                    if (c.waiting.empty()) break;
+                    Slot &sl = ln.slots[d];
+                    if (!sl.batch.empty()) continue;
+                    while (!c.waiting.empty() && (int)sl.batch.size() < max_batch) {
+                        size_t off = 0;
+                        if (!arena.alloc(c.req_bytes, &off)) break;
+                        Request *rq = c.waiting.front();
+                        c.waiting.pop_front();
+                        rq->buf_off = off;
+                        sl.batch.push_back(rq);
+                    }
+                    if (sl.batch.empty()) {   // arena full: retry after a retirement
+                        full = true;
+                        break;
+                    }
+                    lk.unlock();
+                    const int st = launch(c, ln, sl);
+                    if (st != CHY_OK) {   // nothing may still use the buffers
+                        cudaStreamSynchronize(ln.s_in);
+                        cudaStreamSynchronize(ln.stream);
+                        cudaStreamSynchronize(ln.s_out);
+                    }
+                    lk.lock();
+                    if (st != CHY_OK) retire(c, sl, st);
+                    else batches++;
+                    progress = true;
                 }
-                if (ln.batch.empty()) break;   // arena full: retry after a retirement
-                lk.unlock();
-                const int st = launch(c, ln);
-                if (st != CHY_OK) cudaStreamSynchronize(ln.stream);   // nothing may still use the buffers
-                lk.lock();
-                if (st != CHY_OK) retire(c, ln, st);
-                else batches++;
-                progress = true;
-            }
         }
         if (progress) cv_done.notify_all();
         if (stop && incoming.empty()) {
@@ -358,7 +412,7 @@ void chy_server::run()
             for (auto &kv : classes) {
                 if (!kv.second->waiting.empty()) idle = false;
                 for (Lane &ln : kv.second->lanes)
-                    if (!ln.batch.empty()) idle = false;
+                    if (!ln.idle()) idle = false;
             }
             if (idle) break;
         }
@@ -460,11 +514,7 @@ void chy_server_destroy(chy_server *s)
     s->cv_work.notify_one();
     if (s->worker.joinable()) s->worker.join();
     for (auto &kv : s->classes)
-        for (Lane &ln : kv.second->lanes) {
-            if (ln.plan) chy_plan_destroy(ln.plan);
-            if (ln.stream) cudaStreamDestroy(ln.stream);
-            if (ln.done) cudaEventDestroy(ln.done);
-        }
+        for (Lane &ln : kv.second->lanes) lane_free(ln);
     cudaFree(s->arena_base);
     delete s;
 }
