@@ -56,6 +56,10 @@ struct Packer {
 
 }  // namespace
 
+// The calling thread's last-error message, for the other translation units
+// (serve.cu); returns code.
+int chy_internal_fail(int code, const char *msg) { return fail(code, msg); }
+
 static int ensure_host_staging(chy_plan *p);
 
 // getBinaryPosition's circular orbit (radhydro/ExternalRoutines.f:91-105):

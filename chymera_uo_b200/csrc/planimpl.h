@@ -108,6 +108,9 @@ inline cudaError_t copy_phi_rim(double *dst, const double *src, int J, int K, in
     return cudaMemcpy2DAsync(dst + J + 1, plane, src + J + 1, plane, sizeof(double), L, kind, s);
 }
 
+// Sets the calling thread's chy_last_error message; returns code (api.cu).
+int chy_internal_fail(int code, const char *msg);
+
 // One launch sequence over nb device-pointer solves (api.cu).
 int chy_internal_run_batch(chy_plan *p, const chy::BatchPtrs &bp, int nb, cudaStream_t s);
 

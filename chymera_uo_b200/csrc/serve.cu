@@ -424,24 +424,25 @@ extern "C" {
 
 int chy_server_create(const chy_server_opts *o, chy_server **out)
 {
-    if (!out) return CHY_ERR_ARG;
+    if (!out) return chy_internal_fail(CHY_ERR_ARG, "chy_server_create: null output pointer");
     *out = nullptr;
     auto s = std::make_unique<chy_server>();
-    if (cudaGetDevice(&s->device) != cudaSuccess) return CHY_ERR_CUDA;
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return CHY_ERR_CUDA;
-    s->budget = (o && o->hbm_budget > 0) ? (size_t)o->hbm_budget : free_b / 4 * 3;
     s->precision = o ? o->precision : CHY_PREC_MIXED;
-    s->max_batch = (o && o->max_batch > 0) ? std::min(o->max_batch, (int)kMaxBatchPtrs) : 8;
     if (s->precision != CHY_PREC_FP64 && s->precision != CHY_PREC_MIXED && s->precision != CHY_PREC_FP64_BLKTRI)
-        return CHY_ERR_ARG;
+        return chy_internal_fail(CHY_ERR_ARG, "chy_server_create: precision must be CHY_PREC_FP64, _MIXED or _FP64_BLKTRI");
+    if (cudaGetDevice(&s->device) != cudaSuccess) return chy_internal_fail(CHY_ERR_CUDA, "chy_server_create: no device");
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
+        return chy_internal_fail(CHY_ERR_CUDA, "chy_server_create: cudaMemGetInfo failed");
+    s->budget = (o && o->hbm_budget > 0) ? (size_t)o->hbm_budget : free_b / 4 * 3;
+    s->max_batch = (o && o->max_batch > 0) ? std::min(o->max_batch, (int)kMaxBatchPtrs) : 8;
     // request buffers get the arena fraction of the budget; plans the rest
     const double frac = (o && o->arena_fraction > 0.0 && o->arena_fraction < 1.0) ? o->arena_fraction : 0.5;
     const size_t arena = ((size_t)(s->budget * frac)) & ~(size_t)255;
-    if (arena > free_b) return CHY_ERR_NOMEM;
+    if (arena > free_b) return chy_internal_fail(CHY_ERR_NOMEM, "chy_server_create: arena larger than free device memory");
     if (cudaMalloc(&s->arena_base, arena) != cudaSuccess) {
         cudaGetLastError();
-        return CHY_ERR_NOMEM;
+        return chy_internal_fail(CHY_ERR_NOMEM, "chy_server_create: arena allocation failed");
     }
     s->arena.reset(arena);
     chy_server *raw = s.release();

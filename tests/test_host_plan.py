@@ -237,6 +237,12 @@ def test_external_and_source_argument_checks(chylib):
     b = chylib.ChyBinary(1.0, 100.0)
     assert L.chy_plan_set_binary(None, C.byref(b)) == 10
     assert C.sizeof(chylib.ChyTune) == 6 * 4 + 2 * 8 + 8
+    # argument errors come with their own message
+    o = chylib.ServerOpts()
+    o.precision = 7
+    srv = C.c_void_p()
+    assert L.chy_server_create(C.byref(o), C.byref(srv)) == 10
+    assert b"precision" in L.chy_last_error()
     t = chylib.ChyTune()
     assert L.chy_autotune_multi(0, None, None, None, None, 1, C.byref(t)) == 10
     assert L.chy_plan_set_schedule(None, C.byref(t)) == 10
