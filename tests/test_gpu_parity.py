@@ -400,3 +400,43 @@ def test_fp64_paths_against_a_long_double_mode_solution(chylib, ora):
     assert err["fp64"] < 1e-12, err
     assert err["blktri"] < 5e-12, err
     assert err["fp64"] < err["blktri"], err
+
+
+@pytest.mark.parametrize("prec", ["mixed", "blktri"])
+def test_host_copies_read_and_write_only_their_cells(chylib, prec):
+    """Host-pointer solves copy RHO in and PHI out as single linear spans.
+    RHO cells outside the read set RHO(2:JMAX, 2:KMAX, :) -- here NaN -- do
+    not reach the result, and PHI cells outside the write set (PHI(:, KMAX+2, :)
+    and PHI(JMAX+2, 1, :), here random) come back unchanged; the result equals
+    the device-pointer solve of a clean RHO, bit for bit, through a plan and
+    through the server."""
+    import torch
+    J, K, L = 64, 32, 64
+    clean = synth.disk_density(J, K, L, 23, spiral=True, spectrum=True)
+    dirty = clean.copy(order="F")
+    dirty[0, :, :] = np.nan          # RHO(1, :, :)
+    dirty[J:, :, :] = np.nan         # RHO(JMAX+1:JMAX+2, :, :)
+    dirty[:, 0, :] = np.nan          # RHO(:, 1, :)
+    dirty[:, K:, :] = np.nan         # RHO(:, KMAX+1:KMAX+2, :)
+    rng = np.random.default_rng(4)
+    phi0 = np.zeros_like(clean, order="F")
+    phi0[:, K + 1, :] = rng.random((J + 2, L))
+    phi0[J + 1, 0, :] = rng.random(L)
+    plan = chylib.Plan(chylib.grid(J, K, L), prec, 1)
+    ref = plan.solve(chylib.to_cuda_fortran(clean), chylib.to_cuda_fortran(phi0))
+    torch.cuda.synchronize()
+    ref = ref.cpu().numpy()
+    host = plan.solve(dirty, phi0.copy(order="F"))
+    assert np.array_equal(host, ref)
+    assert np.array_equal(host[:, K + 1, :], phi0[:, K + 1, :]) and np.array_equal(host[J + 1, 0, :], phi0[J + 1, 0, :])
+    srv = chylib.Server(prec, hbm_budget=4 << 30, max_batch=2)
+    try:
+        a = chylib.pinned_fortran(dirty.shape)
+        a[...] = dirty
+        f = chylib.pinned_fortran(dirty.shape)
+        f[...] = phi0
+        t = srv.submit(chylib.grid(J, K, L), a, f)
+        srv.wait(t)
+        assert np.array_equal(np.asarray(f), ref)
+    finally:
+        srv.close()
