@@ -23,10 +23,14 @@ def interior(a):
     return a[1:J, 1:K, :]
 
 
-def test_expired_wait_is_reported_and_the_next_solve_is_clean(chylib):
+@pytest.mark.parametrize("mode_kernel", [1, 2])
+def test_expired_wait_is_reported_and_the_next_solve_is_clean(chylib, mode_kernel):
+    """Both fused mode-solve kernels: k_mode_mixed (1) and the CTA pairs of
+    k_mode_pair (2), whose CTAs also end with a cluster barrier."""
     import torch
     rho = synth.disk_density(J, K, L, 9, spiral=True, spectrum=True)
     plan = chylib.Plan(chylib.grid(J, K, L), "mixed", 2)
+    plan.set_schedule(mode_kernel=mode_kernel)
     lib = chylib.lib()
     ref = plan.solve(rho, np.zeros_like(rho, order="F"))
     assert np.all(np.isfinite(ref))
