@@ -739,12 +739,11 @@ def main():
         a[...] = b
     for a in pin_p:
         a[...] = 0.0
-    # the library's copies per solve: RHO from row 2 of the first plane to row
-    # KMAX of the last, PHI's untouched cells in, PHI from PHI(1,1,1) to
-    # PHI(JMAX+2, KMAX+1, LMAX) out (chymera_uo_b200/csrc/planimpl.h)
-    plane = (J + 2) * (K + 2)
-    h2d = B * 8 * ((L - 1) * plane + (K - 1) * (J + 2) + L * (J + 3))
-    d2h = B * 8 * ((L - 1) * plane + (K + 1) * (J + 2))
+    # the library's copies per solve: RHO whole and PHI's untouched cells in,
+    # PHI whole out (chymera_uo_b200/csrc/planimpl.h)
+    vol = (J + 2) * (K + 2) * L
+    h2d = B * 8 * (vol + L * (J + 3))
+    d2h = B * 8 * vol
     ke = max(3, args.steps // 4)
     for _ in range(args.warmup):
         plan.solve_batch(pin_r, pin_p)

@@ -672,8 +672,7 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         for (int i = 0; i < nb; i++) {
             double *dr = base + (size_t)i * 2 * p->nvol, *df = dr + p->nvol;
             const double *hr = rho[first + i];
-            CHY_CUDA(copy_rho_read_set(dr, hr, hp.J, hp.K, hp.L, p->star.on && p->star.indirect ? hp.K : hp.K - 1,
-                                       p->s_h2d));
+            CHY_CUDA(copy_rho_in(dr, hr, hp.J, hp.K, hp.L, p->s_h2d));
             // the cells the solve leaves alone start from the caller's values:
             // the external potential updates them, and the copy out returns
             // them with the rest of PHI
@@ -700,7 +699,7 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         CHY_CUDA(cudaStreamWaitEvent(p->s_d2h, p->ev_done[slot], 0));
         for (int i = 0; i < nb; i++) {
             CHY_CUDA(copy_phi_out(phi[first + i], bp.phi[i], hp.J, hp.K, hp.L, p->s_d2h));
-            // the last plane's row KMAX+2, which the span leaves out
+            // the cells the external potential updated
             if (p->star.on)
                 CHY_CUDA(copy_phi_rim(phi[first + i], bp.phi[i], hp.J, hp.K, hp.L, cudaMemcpyDeviceToHost, p->s_d2h));
         }

@@ -63,36 +63,30 @@ struct chy_plan {
     MixedState *mx = nullptr;
 };
 
-// Host <-> device copies of host-pointer solves are single linear copies:
-// with copies running in both directions at once, pitched (2-D) copies of the
-// same rows reached about 12% less PCIe throughput on B200 hosts.
+// Host <-> device copies of host-pointer solves move whole arrays as single
+// linear copies: with copies running in both directions at once, pitched (2-D)
+// copies of the read and write sets reached about 12% less PCIe throughput on
+// B200 hosts, and linear copies of sub-spans starting inside the array about
+// 9% less, than linear copies of the whole (page-aligned) arrays.
 //
-// Copies one solve's PHI from device to the caller's host array as one span,
-// PHI(1,1,1) .. PHI(JMAX+2, KMAX+1, LMAX): the write set (PHI(1:JMAX+1, 1, :)
-// and PHI(:, 2:KMAX+1, :)) and, between its pieces, the cells a solve never
-// writes (PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :), all but the last plane's
-// row KMAX+2).  Those cells of the device copy hold the caller's own values,
-// copied in by copy_phi_rim earlier in the same call, so the host gets them
-// back unchanged.
+// Copies one solve's PHI from device to the caller's host array, whole: the
+// write set (PHI(1:JMAX+1, 1, :) and PHI(:, 2:KMAX+1, :)) and the cells a solve
+// never writes (PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :)).  Those cells of the
+// device copy hold the caller's own values, copied in by copy_phi_rim earlier
+// in the same call, so the host gets them back unchanged.
 inline cudaError_t copy_phi_out(double *host, const double *dev, int J, int K, int L, cudaStream_t s)
 {
-    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2;
-    const size_t n = (size_t)(L - 1) * J2 * K2 + ((size_t)K + 1) * J2;
+    const size_t n = ((size_t)J + 2) * ((size_t)K + 2) * (size_t)L;
     return cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, s);
 }
 
-// Copies the rows of RHO a solve reads, RHO(:, 2:nrows+1, :), from the
-// caller's host array to a device copy of the whole volume; the other rows of
-// the device copy are never read.  A solve reads RHO(2:JMAX, 2:KMAX, :)
-// (nrows = KMAX-1); the INDIRECT star shift also reads row KMAX+1 (nrows = KMAX).
-inline cudaError_t copy_rho_read_set(double *dev, const double *host, int J, int K, int L, int nrows,
-                                     cudaStream_t s)
+// Copies one solve's RHO from the caller's host array to the device, whole
+// (a solve reads RHO(2:JMAX, 2:KMAX, :); the INDIRECT star shift also row
+// KMAX+1; no kernel reads the other cells).
+inline cudaError_t copy_rho_in(double *dev, const double *host, int J, int K, int L, cudaStream_t s)
 {
-    // one span from row 2 of the first plane to row nrows+1 of the last: the
-    // rows in between planes come along, and no solve reads them
-    const size_t J2 = (size_t)J + 2, K2 = (size_t)K + 2;
-    const size_t n = (size_t)(L - 1) * J2 * K2 + (size_t)nrows * J2;
-    return cudaMemcpyAsync(dev + J2, host + J2, n * sizeof(double), cudaMemcpyHostToDevice, s);
+    const size_t n = ((size_t)J + 2) * ((size_t)K + 2) * (size_t)L;
+    return cudaMemcpyAsync(dev, host, n * sizeof(double), cudaMemcpyHostToDevice, s);
 }
 
 // Copies the cells of PHI that a solve never writes, PHI(:, KMAX+2, :) and

@@ -287,7 +287,7 @@ int chy_server::launch(SizeClass &c, Lane &ln, Slot &sl)
     for (int i = 0; i < nb; i++) {
         Request *rq = sl.batch[i];
         double *dr = reinterpret_cast<double *>(arena_base + rq->buf_off), *df = dr + c.nvol;
-        if (copy_rho_read_set(dr, rq->rho, c.J, c.K, c.L, c.K - 1, ln.s_in) != cudaSuccess) return CHY_ERR_CUDA;
+        if (copy_rho_in(dr, rq->rho, c.J, c.K, c.L, ln.s_in) != cudaSuccess) return CHY_ERR_CUDA;
         // the cells the solve leaves alone go back with the rest of PHI
         if (copy_phi_rim(df, rq->phi, c.J, c.K, c.L, cudaMemcpyHostToDevice, ln.s_in) != cudaSuccess)
             return CHY_ERR_CUDA;
