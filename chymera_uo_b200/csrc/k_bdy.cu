@@ -31,12 +31,14 @@ __global__ void __launch_bounds__(kSubThreads) k_bdy_sub(DevTables t, Work w, in
     const int RL = t.srow, NT_ = t.ntrm, per = 2 * t.ncol;
     double *s_row = smem;                                      // [ns][RL]: TERM, r^-(2l+1), DV
     double *s_mom = smem + kSubChunk * RL;                     // [spp][ns][21]
+    int *s_ring = reinterpret_cast<int *>(s_mom + (size_t)spp * kSubChunk * 21);   // [ns] ring index
     const int sc = blockIdx.x;
     const int s0 = t.sub_start[sc], s1 = t.sub_start[sc + 1], ns = s1 - s0;
 
     // per ring, geometry from the plan (TERM(I) of pot/boundary.f:385-502,
     // r^-(2l+1) of :587, DV of :516)
     for (int i = threadIdx.x; i < ns * RL; i += blockDim.x) s_row[i] = t.sterm[(size_t)s0 * RL + i];
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) s_ring[i] = t.ring_sorted[s0 + i];
     const int b0 = blockIdx.z * kSubBatch, b1 = min(nb, b0 + kSubBatch);
     for (int b = b0; b < b1; b += spp) {
         const int nsl = min(spp, b1 - b);
@@ -45,8 +47,7 @@ __global__ void __launch_bounds__(kSubThreads) k_bdy_sub(DevTables t, Work w, in
         for (int it = threadIdx.x; it < nsl * ns * 21; it += blockDim.x) {
             const int sl = it / (ns * 21), rq = it % (ns * 21), r = rq / 21, q = rq % 21;
             const double *mom = w.mom + (size_t)(b + sl) * w.smom;
-            s_mom[((size_t)sl * kSubChunk + r) * 21 + q] =
-                s_row[r * RL + NT_ + 11] * mom[(size_t)q * t.nring + t.ring_sorted[s0 + r]];
+            s_mom[((size_t)sl * kSubChunk + r) * 21 + q] = s_row[r * RL + NT_ + 11] * mom[(size_t)q * t.nring + s_ring[r]];
         }
         __syncthreads();
         for (int task = threadIdx.x; task < nsl * per; task += blockDim.x) {
@@ -55,13 +56,29 @@ __global__ void __launch_bounds__(kSubThreads) k_bdy_sub(DevTables t, Work w, in
             const int term = t.col_term[col], m = t.col_m[col], l = t.col_l[col];
             const int mq = t.col_part[col] == 0 ? m : 10 + m;
             const double *sm = s_mom + (size_t)sl * kSubChunk * 21;
-            double acc = 0.0;
+            // four partial sums (rings 4i .. 4i+3 into a0 .. a3, a remainder
+            // into a0), then (a0 + a1) + (a2 + a3): a fixed order with a
+            // quarter of the dependent chain
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            int r = 0;
             if (!out) {
-                for (int r = 0; r < ns; ++r) acc = acc + s_row[r * RL + term] * sm[r * 21 + mq];
+                for (; r + 4 <= ns; r += 4) {
+                    a0 = a0 + s_row[r * RL + term] * sm[r * 21 + mq];
+                    a1 = a1 + s_row[(r + 1) * RL + term] * sm[(r + 1) * 21 + mq];
+                    a2 = a2 + s_row[(r + 2) * RL + term] * sm[(r + 2) * 21 + mq];
+                    a3 = a3 + s_row[(r + 3) * RL + term] * sm[(r + 3) * 21 + mq];
+                }
+                for (; r < ns; ++r) a0 = a0 + s_row[r * RL + term] * sm[r * 21 + mq];
             } else {
-                for (int r = 0; r < ns; ++r)
-                    acc = acc + (s_row[r * RL + term] * sm[r * 21 + mq]) * s_row[r * RL + NT_ + l];
+                for (; r + 4 <= ns; r += 4) {
+                    a0 = a0 + (s_row[r * RL + term] * sm[r * 21 + mq]) * s_row[r * RL + NT_ + l];
+                    a1 = a1 + (s_row[(r + 1) * RL + term] * sm[(r + 1) * 21 + mq]) * s_row[(r + 1) * RL + NT_ + l];
+                    a2 = a2 + (s_row[(r + 2) * RL + term] * sm[(r + 2) * 21 + mq]) * s_row[(r + 2) * RL + NT_ + l];
+                    a3 = a3 + (s_row[(r + 3) * RL + term] * sm[(r + 3) * 21 + mq]) * s_row[(r + 3) * RL + NT_ + l];
+                }
+                for (; r < ns; ++r) a0 = a0 + (s_row[r * RL + term] * sm[r * 21 + mq]) * s_row[r * RL + NT_ + l];
             }
+            const double acc = (a0 + a1) + (a2 + a3);
             w.sub[(size_t)(b + sl) * w.ssub + (size_t)sc * 2 * t.ncol + (size_t)out * t.ncol + col] = acc;
         }
     }
@@ -123,7 +140,7 @@ cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStrea
     // at most half the block
     const int per = 2 * t.ncol, spp = (nb >= 2 && 2 * per <= kSubThreads) ? 2 : 1;
     const int threads = spp == 2 ? ((2 * per + 31) / 32) * 32 : 256;
-    const size_t sm = (size_t)kSubChunk * (t.srow + 21 * spp) * sizeof(double);
+    const size_t sm = (size_t)kSubChunk * (t.srow + 21 * spp) * sizeof(double) + (size_t)kSubChunk * sizeof(int);
     cudaError_t e = ensure_smem((const void *)k_bdy_sub, sm);
     if (e != cudaSuccess) return e;
     k_bdy_sub<<<dim3(t.nsub, 1, (nb + kSubBatch - 1) / kSubBatch), threads, sm, s>>>(t, w, nb, spp);
