@@ -121,6 +121,9 @@ struct MixedState {
     bool paired = false;            // the last mode solve ran k_mode_pair (per-half sums)
     CUtensorMap tm_x{};             // X as rows of JMAX doubles: 16 x KMAX tiles, 128-byte swizzle
     CUtensorMap tm_xs{};            // the same with 16 x (KMAX-1) tiles: stores skip the boundary row
+    CUtensorMap tm_pl{};            // k_mode_pair, one warp's rows: 16 x min(KMAX, 32) tiles
+    CUtensorMap tm_ps{};            // its stores: 16 x 32 tiles
+    CUtensorMap tm_psl{};           // the last warp's stores: 16 x (KMAX-1 - 32 (ceil((KMAX-1)/32) - 1))
     bool tm_ok = false;
 };
 
@@ -932,11 +935,14 @@ __global__ void __launch_bounds__(256, 1) k_mode_mixed(DevTables t, Work w, Mixe
             mma_pend = false;
             tc_fence_after();
             float *cvs = reinterpret_cast<float *>(sBh);   // [j][p] multipliers for the back sweeps
-            if (tid == 0) {
-                // B tile free: this m's multipliers for the back sweeps
+            if (lane == 0 && (warp & 1) == 0) {
+                // B tile free: this m's multipliers for the back sweeps, a
+                // quarter per even warp (an issuing thread waits while the
+                // copy engine takes in its bytes, so no warp takes all four)
+                const int q = warp >> 1;
                 const float *src = x.sw_mul + (size_t)m * NT * 128;
-                mbar_expect_tx(bar_cv, (uint32_t)NT * 512);
-                for (int q = 0; q < 4; ++q) bulk_g2s(cvs + q * NT * 32, src + q * NT * 32, (uint32_t)NT * 128, bar_cv);
+                if (q == 0) mbar_expect_tx(bar_cv, (uint32_t)NT * 512);
+                bulk_g2s(cvs + q * NT * 32, src + q * NT * 32, (uint32_t)NT * 128, bar_cv);
             }
             cv_pend = true;
             // ---- radial sweeps (T_r(m) + lam_p) w = W_p, top-down over rows
@@ -1267,10 +1273,10 @@ struct PairSmem {
     static constexpr size_t ft = bn + 128 * 8;                      // float4 [128] {0, AM, CM, 0}
     static constexpr size_t dred = ft + 128 * 16;                   // double [2][24]
     static constexpr size_t fred = dred + 2 * 24 * 8;               // float [2][8]
-    static constexpr size_t edge = fred + 2 * 8 * 4;                // float [2][2][4][32]
-    static constexpr size_t xch = edge + 2 * 2 * 4 * 32 * 4;        // float4 [2][2][128] incoming exchanges
-    static constexpr size_t bars = xch + 2 * 2 * 128 * 16;          // uint64 [1 + 2 * 9]
-    static constexpr size_t misc = bars + 19 * 8;                   // tmem slot, flags [2]
+    static constexpr size_t edge = fred + 2 * 8 * 4;                // float [2][4][2][128] x0 edge rows
+    static constexpr size_t xch = edge + 2 * 4 * 2 * 128 * 4;       // float4 [2][2][128] incoming exchanges
+    static constexpr size_t bars = xch + 2 * 2 * 128 * 16;          // uint64 [3 + 2 * 20]
+    static constexpr size_t misc = bars + 43 * 8;                   // tmem slot, flags [2]
     static constexpr size_t bytes = misc + 16;
 };
 static_assert(PairSmem::bytes <= 227 * 1024, "pair shared memory");
@@ -1333,8 +1339,9 @@ __device__ __forceinline__ void cluster_sync_all()
 }
 
 __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, MixedDev x, int nb,
-                                                      const __grid_constant__ CUtensorMap tm_x,
-                                                      const __grid_constant__ CUtensorMap tm_xs)
+                                                      const __grid_constant__ CUtensorMap tm_l,
+                                                      const __grid_constant__ CUtensorMap tm_s,
+                                                      const __grid_constant__ CUtensorMap tm_sl)
 {
     extern __shared__ __align__(1024) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1352,12 +1359,15 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
     float4 *f_t = reinterpret_cast<float4 *>(sm + PairSmem::ft);
     double *d_red = reinterpret_cast<double *>(sm + PairSmem::dred) + g * 24;
     float *f_red = reinterpret_cast<float *>(sm + PairSmem::fred) + g * 8;
-    float *f_edge = reinterpret_cast<float *>(sm + PairSmem::edge) + g * 256;
+    // x0's edge rows of this group: [warp][top (lane 0), bottom (lane 31)][column]
+    float *f_edge = reinterpret_cast<float *>(sm + PairSmem::edge) + g * 1024;
     float4 *xch = reinterpret_cast<float4 *>(sm + PairSmem::xch) + g * 256;   // [2 slots][128]
     uint64_t *bar_a = reinterpret_cast<uint64_t *>(sm + PairSmem::bars);
-    uint64_t *gb = bar_a + 1 + g * 9;                   // this group's barriers
-    uint64_t *bar_mma = gb, *bar_ring = gb + 1, *bar_cv = gb + 5, *bar_x = gb + 6;   // bar_x[2]
-    uint64_t *bar_stagger = bar_a + 9;                  // group 0's gb[8]: group 1 may start
+    uint64_t *bar_stagger = bar_a + 1;                  // group 1 may start
+    uint64_t *bar_probe = bar_a + 2;                    // nothing arrives on it (test hook)
+    uint64_t *gb = bar_a + 3 + g * 20;                  // this group's barriers
+    uint64_t *bar_mma = gb, *bar_cv = gb + 1, *bar_x = gb + 2;   // bar_x[2]
+    uint64_t *bar_ring = gb + 4 + 4 * (warp & 3);       // this warp's four ring slots
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(sm + PairSmem::misc);
     int *s_flag = reinterpret_cast<int *>(sm + PairSmem::misc + 8) ;   // [2]
 
@@ -1366,8 +1376,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        mbar_init(bar_a, 1);
-        for (int i = 0; i < 18; ++i) mbar_init(bar_a + 1 + i, 1);
+        for (int i = 0; i < 43; ++i) mbar_init(bar_a + i, 1);
         s_flag[0] = s_flag[1] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -1411,7 +1420,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
     if (x.probe_polls > 0) {
         // test hook: a bounded wait on a barrier nothing arrives on, before
         // anything is issued
-        if (tid == 0 && !mbar_wait_n(bar_a + 18, 0, x.probe_polls)) s_flag[0] = s_flag[1] = 1;
+        if (tid == 0 && !mbar_wait_n(bar_probe, 0, x.probe_polls)) s_flag[0] = s_flag[1] = 1;
         __syncthreads();
         failed = s_flag[g] != 0;
         a_wait = a_wait && !failed;
@@ -1490,44 +1499,74 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
             const uint32_t acc = G + (res_x ? 128u : 0u);   // product / sweep columns
             const uint32_t rcol = G + 128u;                 // residual columns
             // ---- residual r = d_k (Y - A_m x) (FP64) -> TMEM as FP32, this
-            // CTA's columns in 16-column tiles through a four-slot ring
+            // CTA's columns in 16-column tiles through a four-slot ring.  Each
+            // warp loads, reads and recycles only its own 32 rows of a slot
+            // (one tensor-map box per warp and tile, one mbarrier per warp and
+            // slot), so the warps of the group never wait for one another in
+            // this loop: an issuing thread waits while the copy engine takes
+            // in its bytes, and every warp now pays that for its own 4 KB
+            const int quad = warp & 3;
+            const bool wrows = 32 * quad < K;               // this warp's rows hold data
             auto issue = [&](int c) {
-                if (c >= nch) return;
+                if (c >= nch || !wrows) return;
                 const int sl = c % kPairRing;
                 ring_pend |= 1u << sl;
-                if (warp != 4 * g) return;
-                uint8_t *slot = sB + sl * kPairTileB;
+                uint8_t *slot = sB + sl * kPairTileB + quad * 4096;
                 const int x0c = col0 + 16 * c;
                 if (x0c < J) {
                     if (lane == 0) {
-                        mbar_expect_tx(bar_ring + sl, (uint32_t)(K * 128));
-                        tma_load_2d(slot, &tm_x, x0c, row0, bar_ring + sl);
+                        fence_proxy_async();
+                        mbar_expect_tx(bar_ring + sl, (uint32_t)(min(K, 32) * 128));
+                        tma_load_2d(slot, &tm_l, x0c, row0 + 32 * quad, bar_ring + sl);
                     }
                 } else {
-                    for (int i = lane; i < K * 16; i += 32) reinterpret_cast<double *>(slot)[i] = 0.0;
+                    for (int i = lane; i < 32 * 16; i += 32) reinterpret_cast<double *>(slot)[i] = 0.0;
                     __syncwarp();
                     if (lane == 0) mbar_arrive(bar_ring + sl);
                 }
             };
+            bool wbad = false;                              // a wait of this warp ran out
             auto landed = [&](int c) {
+                if (!wrows) return;
                 const int sl = c % kPairRing;
                 if (mbar_wait(bar_ring + sl, (ring_ph >> sl) & 1u)) {
                     ring_ph ^= 1u << sl;
                     ring_pend &= ~(1u << sl);
                 } else {
                     s_flag[g] = 1;
+                    wbad = true;
                 }
             };
             auto at = [&](const uint8_t *slot, int k, int q) -> const double * {
                 return reinterpret_cast<const double *>(slot + k * 128 + ((((q >> 1) ^ (k & 7))) << 4) + ((q & 1) << 3));
             };
-            fence_proxy_async();
-            gbar();
-            for (int c = 0; c < kPairRing - 1; ++c) issue(c);
-            const int k = kq, quad = warp & 3;
+            const int k = kq;
             const bool krow = k < NZ;
             const double bnk = d_bn[k];
             float rmax = 0.0f;
+            if (res_x) {
+                // x0's top and bottom rows of every warp for the vertical
+                // neighbours across warps, staged once for all chunks
+                float *my = f_edge + quad * 256;
+                for (int c0 = 0; c0 < NH; c0 += 32) {
+                    float v[32];
+                    tm_ld32(tmem + lane_base + G + c0, v);
+                    if (lane == 0) {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) my[c0 + u] = v[u];
+                    }
+                    if (lane == 31) {
+#pragma unroll
+                        for (int u = 0; u < 32; ++u) my[128 + c0 + u] = v[u];
+                    }
+                }
+            }
+            fence_proxy_async();
+            gbar();
+            for (int c = 0; c < kPairRing - 1; ++c) issue(c);
+            const float *eu = f_edge + (quad > 0 ? quad - 1 : quad) * 256 + 128;   // row 32 quad - 1
+            const float *ed = f_edge + (quad < 3 ? quad + 1 : quad) * 256;         // row 32 quad + 32
+            const float zu = quad > 0 ? 1.f : 0.f, zd = quad < 3 ? 1.f : 0.f;
             for (int c = 0; c < nch; ++c) {
                 const int c0 = 16 * c;
                 float xc[16], xlf = 0.f, xrt = 0.f;
@@ -1538,20 +1577,12 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
                     tm_ld1_nw(tmem + lane_base + G + (uint32_t)(jr < NH ? jr : NH - 1), xrt);
                     landed(c);
                     tm_wait_ld18(xc, xlf, xrt);
-                    float *ed = f_edge + ((c & 1) * 4 + quad) * 32;
-                    if (lane == 0) {
-#pragma unroll
-                        for (int u = 0; u < 16; ++u) ed[u] = xc[u];
-                    }
-                    if (lane == 31) {
-#pragma unroll
-                        for (int u = 0; u < 16; ++u) ed[16 + u] = xc[u];
-                    }
                 } else {
                     landed(c);
                 }
-                gbar();
-                if (s_flag[g]) break;
+                if (wbad) break;
+                // this warp's rows of the slot of chunk c - 1 are read: reuse it
+                __syncwarp();
                 issue(c + kPairRing - 1);
                 const uint8_t *slot = sB + (c % kPairRing) * kPairTileB;
                 double yv[16];
@@ -1579,10 +1610,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
                 }
                 float v[16];
                 if (res_x) {
-                    const float *eu = f_edge + ((c & 1) * 4 + (quad > 0 ? quad - 1 : quad)) * 32 + 16;
-                    const float *ed = f_edge + ((c & 1) * 4 + (quad < 3 ? quad + 1 : quad)) * 32;
                     const bool top0 = lane == 0, bot31 = lane == 31;
-                    const float zu = quad > 0 ? 1.f : 0.f, zd = quad < 3 ? 1.f : 0.f;
                     double xd_[18];
                     // the neighbours across the pair's column boundary come from the peer
                     xd_[0] = c0 == 0 ? (rank == 1 ? edge_in : 0.0) : (double)xlf;
@@ -1594,7 +1622,7 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
                         const int jl = c0 + u, j = col0 + jl;
                         float xu = __shfl_up_sync(0xffffffffu, xc[u], 1);
                         float xd = __shfl_down_sync(0xffffffffu, xc[u], 1);
-                        const float eu_u = eu[u] * zu, ed_u = ed[u] * zd;
+                        const float eu_u = eu[jl] * zu, ed_u = ed[jl] * zd;
                         xu = top0 ? eu_u : xu;
                         xd = bot31 ? ed_u : xd;
                         double ax = (bnk + d_bm[jl]) * xd_[u + 1];
@@ -1619,12 +1647,12 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
                 tm_st16_nw(tmem + lane_base + rcol + c0, v);
             }
             tm_wait_st();
-            if (s_flag[g]) { failed = true; break; }
             if (!stag_sent && it == nit - 1) {
                 if (gt == 0) mbar_arrive(bar_stagger);
                 stag_sent = true;
             }
             const int k1 = pow2_exp(group_max(rmax));
+            if (s_flag[g]) { failed = true; break; }
             const float s1 = ldexpf(1.0f, k1);
             // ---- TMEM r -> B tile (row j, K index k), FP16 hi/lo
             for (int c0 = 0; c0 < NH; c0 += 32) {
@@ -1654,10 +1682,14 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
             mma_pend = false;
             tc_fence_after();
             float *cvs = reinterpret_cast<float *>(sB);   // [local row][p] multipliers
-            if (gt == 0) {
+            if (lane == 0) {
+                // a quarter of the multipliers per warp of the group (an
+                // issuing thread waits while the copy engine takes in its
+                // bytes, so no warp takes all four)
+                const int q = warp & 3;
                 const float *src = x.sw_mul + ((size_t)m * NT + col0) * 128;
-                mbar_expect_tx(bar_cv, (uint32_t)NH * 512);
-                for (int q = 0; q < 4; ++q) bulk_g2s(cvs + q * NH * 32, src + q * NH * 32, (uint32_t)NH * 128, bar_cv);
+                if (q == 0) mbar_expect_tx(bar_cv, (uint32_t)NH * 512);
+                bulk_g2s(cvs + q * NH * 32, src + q * NH * 32, (uint32_t)NH * 128, bar_cv);
             }
             cv_pend = true;
             // ---- radial sweeps (T_r(m) + lam_p) w = W_p on this CTA's rows:
@@ -1795,15 +1827,22 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
             }
             // ---- X = x0 + delta (FP64), staged as 16-column tiles (128-byte
             // swizzle) and written by the copy engine as rows 0..KMAX-2 (the
-            // boundary row is not written); column M carries X's own value back
+            // boundary row is not written); column M carries X's own value
+            // back.  Each warp stages and stores its own 32 rows (the last
+            // warp with data one row fewer), so no group barrier is needed
             double sd = 0.0, sx = 0.0;
             const double uk = unscale * ek, u0k = u0 * ek;     // this row's 1/d_k
+            const int srows = min(32, K - 1 - 32 * quad);
+            const CUtensorMap *smap = srows == 32 ? &tm_s : &tm_sl;
             float dv[16], xv[16];
             tm_ld16_nw(tmem + lane_base + acc, dv);
             tm_ld16_nw(tmem + lane_base + G, xv);   // x0 (unused after a single solve)
             for (int c = 0; c < nch; ++c) {
                 const int c0 = 16 * c;
                 uint8_t *slot = sB + (c % kPairStage) * kPairTileB;
+                // this warp's store of the slot's previous chunk has read it
+                if (lane == 0) bulk_wait_read<kPairStage - 1>();
+                __syncwarp();
                 tm_wait_ld32(dv, xv);
                 double xn[16];
 #pragma unroll
@@ -1817,23 +1856,22 @@ __global__ void __launch_bounds__(256, 1) k_mode_pair(DevTables t, Work w, Mixed
                     }
                     if (j == M) xn[u] = ym_keep;        // column M (uniform in the warp)
                 }
+                if (c + 1 < nch) {
+                    tm_ld16_nw(tmem + lane_base + acc + c0 + 16, dv);
+                    tm_ld16_nw(tmem + lane_base + G + c0 + 16, xv);
+                }
 #pragma unroll
                 for (int u = 0; u < 16; u += 2)
                     *reinterpret_cast<double2 *>(slot + kq * 128 + (((u >> 1) ^ (kq & 7)) << 4)) =
                         make_double2(xn[u], xn[u + 1]);
                 fence_proxy_async();
-                if (gt == 0) bulk_wait_read<kPairStage - 2>();   // the slot's previous store has read it
-                gbar();
-                if (c + 1 < nch) {
-                    tm_ld16_nw(tmem + lane_base + acc + c0 + 16, dv);
-                    tm_ld16_nw(tmem + lane_base + G + c0 + 16, xv);
-                }
-                if (gt == 0 && col0 + c0 < J) {
-                    tma_store_2d(&tm_xs, col0 + c0, row0, slot);
+                __syncwarp();
+                if (lane == 0 && srows > 0 && col0 + c0 < J) {
+                    tma_store_2d(smap, col0 + c0, row0 + 32 * quad, slot + quad * 4096);
                     bulk_commit();
                 }
             }
-            if (gt == 0) bulk_wait_all();               // tiles written, staging free for the next item
+            if (lane == 0) bulk_wait_all();             // tiles written, staging free for the next item
             // per-half sums (the host adds the two halves)
             sd = warp_sum(sd);
             sx = warp_sum(sx);
@@ -2378,6 +2416,20 @@ void chy_mixed_bind_work(chy_plan *p, double *base)
                            enc(&p->mx->tm_xs, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p->w.X, dims, strides, box_s, es,
                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+            // k_mode_pair's per-warp boxes (rows 32 q .. 32 q + 31 of an item)
+            const int nsw = (hp.K - 1 + 31) / 32, last = hp.K - 1 - 32 * (nsw - 1);
+            const cuuint32_t box_pl[2] = {16, (cuuint32_t)std::min(hp.K, 32)}, box_ps[2] = {16, 32},
+                             box_psl[2] = {16, (cuuint32_t)last};
+            p->mx->tm_ok = p->mx->tm_ok &&
+                           enc(&p->mx->tm_pl, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p->w.X, dims, strides, box_pl, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+                           enc(&p->mx->tm_ps, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p->w.X, dims, strides, box_ps, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS &&
+                           enc(&p->mx->tm_psl, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, p->w.X, dims, strides, box_psl, es,
+                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         }
     }
 }
@@ -2464,7 +2516,7 @@ int chy_mixed_solve(chy_plan *p, int nb, cudaStream_t s, int *launches)
             cfg.stream = s;
             cfg.attrs = at;
             cfg.numAttrs = 1;
-            if (cudaLaunchKernelEx(&cfg, k_mode_pair, p->t, p->w, d, nb, p->mx->tm_x, p->mx->tm_xs) != cudaSuccess)
+            if (cudaLaunchKernelEx(&cfg, k_mode_pair, p->t, p->w, d, nb, p->mx->tm_pl, p->mx->tm_ps, p->mx->tm_psl) != cudaSuccess)
                 return CHY_ERR_CUDA;
             ms.paired = true;
             *launches = 1;
