@@ -779,6 +779,21 @@ def main():
         accuracy["rel_l2_fp64_vs_oracle_max"] = max(rel_l2(a[ws_sl], b[ws_sl]) for a, b in zip(g64, outs))
         accuracy["rel_l2_fp64_eigen_vs_oracle_max"] = max(rel_l2(a[ws_sl], b[ws_sl]) for a, b in zip(geg, outs))
         accuracy["oracle_solves_compared"] = len(outs)
+        if args.precision == "mixed":
+            # the error against the oracle after each refinement step: 0 = the
+            # first approximate solve alone, 1 = one FP64 correction (the
+            # default), 2 = two
+            per_step = {}
+            nr = min(2, len(outs))
+            for r in (0, 1, 2):
+                pr = chy.Plan(chy.grid(J, K, L), "mixed", nr)
+                pr.set_refine(r)
+                o = [chy.fortran_zeros_cuda(p.shape) for p in phis[:nr]]
+                pr.solve_batch(rhos[:nr], o)
+                torch.cuda.synchronize()
+                per_step[str(r)] = max(rel_l2(a.cpu().numpy()[ws_sl], b[ws_sl]) for a, b in zip(o, outs[:nr]))
+                pr.close()
+            accuracy["rel_l2_mixed_vs_oracle_per_refinement"] = per_step
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
