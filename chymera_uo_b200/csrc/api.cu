@@ -669,19 +669,28 @@ extern "C" int chy_solve_batch(chy_plan *p, int n, const double *const *rho, dou
         double *base = p->stage + (size_t)slot * c * 2 * p->nvol;
         if (used[slot]) CHY_CUDA(cudaStreamWaitEvent(p->s_h2d, p->ev_out[slot], 0));
         BatchPtrs bp{};
+        const double *mapped[kMaxBatchPtrs] = {};
         for (int i = 0; i < nb; i++) {
             double *dr = base + (size_t)i * 2 * p->nvol, *df = dr + p->nvol;
             const double *hr = rho[first + i];
             CHY_CUDA(copy_rho_in(dr, hr, hp.J, hp.K, hp.L, p->s_h2d));
             // the cells the solve leaves alone start from the caller's values:
             // the external potential updates them, and the copy out returns
-            // them with the rest of PHI
-            CHY_CUDA(copy_phi_rim(df, phi[first + i], hp.J, hp.K, hp.L, cudaMemcpyHostToDevice, p->s_h2d));
+            // them with the rest of PHI.  From pinned (mapped) host memory a
+            // kernel reads them below; otherwise the copy engine moves them
+            mapped[i] = chy_internal_mapped_view(phi[first + i]);
+            if (!mapped[i])
+                CHY_CUDA(copy_phi_rim(df, phi[first + i], hp.J, hp.K, hp.L, cudaMemcpyHostToDevice, p->s_h2d));
             bp.rho[i] = dr;
             bp.phi[i] = df;
         }
         CHY_CUDA(cudaEventRecord(p->ev_in[slot], p->s_h2d));
         CHY_CUDA(cudaStreamWaitEvent(s, p->ev_in[slot], 0));
+        for (int i = 0; i < nb; i++)
+            if (mapped[i]) {
+                CHY_CUDA(chy_internal_rim_in(bp.phi[i], mapped[i], hp.J, hp.K, hp.L, s));
+                p->launches += 1;
+            }
         // COEF cells the solve leaves alone (X1 = 0, pot/pot3.f:106) keep the
         // caller's values: the device buffer starts from the host array
         if (p->coef_host)
@@ -959,6 +968,32 @@ extern "C" int chy_autotune_multi(int n, chy_plan *const *plans, const double *c
 }
 
 int chy_internal_run_batch(chy_plan *p, const BatchPtrs &bp, int nb, cudaStream_t s) { return run_batch(p, bp, nb, s); }
+
+const double *chy_internal_mapped_view(const double *host)
+{
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost && a.devicePointer ? static_cast<const double *>(a.devicePointer) : nullptr;
+}
+
+// PHI(:, KMAX+2, L) and PHI(JMAX+2, 1, L) of plane L = blockIdx.x, from the
+// caller's mapped host array (reads cross PCIe) into the device copy.
+__global__ void __launch_bounds__(256) k_phi_rim_in(double *dst, const double *src, int J, int K)
+{
+    const size_t J2 = (size_t)J + 2, plane = J2 * ((size_t)K + 2), base = (size_t)blockIdx.x * plane;
+    const size_t top = base + J2 * ((size_t)K + 1);
+    for (size_t j = threadIdx.x; j < J2; j += blockDim.x) dst[top + j] = src[top + j];
+    if (threadIdx.x == 0) dst[base + J + 1] = src[base + J + 1];
+}
+
+cudaError_t chy_internal_rim_in(double *dev, const double *src, int J, int K, int L, cudaStream_t s)
+{
+    k_phi_rim_in<<<L, 256, 0, s>>>(dev, src, J, K);
+    return cudaGetLastError();
+}
 
 extern "C" int chy_solve(chy_plan *p, const double *rho, double *phi, chy_diag *diag, int ptr_kind,
                          void *stream)

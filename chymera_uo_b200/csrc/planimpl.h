@@ -72,8 +72,9 @@ struct chy_plan {
 // Copies one solve's PHI from device to the caller's host array, whole: the
 // write set (PHI(1:JMAX+1, 1, :) and PHI(:, 2:KMAX+1, :)) and the cells a solve
 // never writes (PHI(:, KMAX+2, :) and PHI(JMAX+2, 1, :)).  Those cells of the
-// device copy hold the caller's own values, copied in by copy_phi_rim earlier
-// in the same call, so the host gets them back unchanged.
+// device copy hold the caller's own values, brought in earlier in the same call
+// (by chy_internal_rim_in from pinned host memory, else by copy_phi_rim), so
+// the host gets them back unchanged.
 inline cudaError_t copy_phi_out(double *host, const double *dev, int J, int K, int L, cudaStream_t s)
 {
     const size_t n = ((size_t)J + 2) * ((size_t)K + 2) * (size_t)L;
@@ -101,6 +102,17 @@ inline cudaError_t copy_phi_rim(double *dst, const double *src, int J, int K, in
     if (e != cudaSuccess) return e;
     return cudaMemcpy2DAsync(dst + J + 1, plane, src + J + 1, plane, sizeof(double), L, kind, s);
 }
+
+// The device-visible address of a caller's host array when it is pinned and
+// mapped (cudaMallocHost / cudaHostAlloc memory under unified addressing),
+// else nullptr (api.cu).
+const double *chy_internal_mapped_view(const double *host);
+
+// The cells of PHI a solve never writes, read by a kernel on `s` from the
+// caller's mapped host array `src` (see chy_internal_mapped_view) into the
+// device copy: the same cells copy_phi_rim moves, without the copy engine's
+// hundreds of small row transfers per solve (api.cu).
+cudaError_t chy_internal_rim_in(double *dev, const double *src, int J, int K, int L, cudaStream_t s);
 
 // Sets the calling thread's chy_last_error message; returns code (api.cu).
 int chy_internal_fail(int code, const char *msg);

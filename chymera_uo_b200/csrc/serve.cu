@@ -284,18 +284,24 @@ int chy_server::launch(SizeClass &c, Lane &ln, Slot &sl)
 {
     BatchPtrs bp{};
     const int nb = (int)sl.batch.size();
+    const double *mapped[kMaxBatchPtrs] = {};
     for (int i = 0; i < nb; i++) {
         Request *rq = sl.batch[i];
         double *dr = reinterpret_cast<double *>(arena_base + rq->buf_off), *df = dr + c.nvol;
         if (copy_rho_in(dr, rq->rho, c.J, c.K, c.L, ln.s_in) != cudaSuccess) return CHY_ERR_CUDA;
-        // the cells the solve leaves alone go back with the rest of PHI
-        if (copy_phi_rim(df, rq->phi, c.J, c.K, c.L, cudaMemcpyHostToDevice, ln.s_in) != cudaSuccess)
+        // the cells the solve leaves alone go back with the rest of PHI: read
+        // by a kernel from pinned (mapped) host memory, else copied
+        mapped[i] = chy_internal_mapped_view(rq->phi);
+        if (!mapped[i] && copy_phi_rim(df, rq->phi, c.J, c.K, c.L, cudaMemcpyHostToDevice, ln.s_in) != cudaSuccess)
             return CHY_ERR_CUDA;
         bp.rho[i] = dr;
         bp.phi[i] = df;
     }
     if (cudaEventRecord(sl.in, ln.s_in) != cudaSuccess || cudaStreamWaitEvent(ln.stream, sl.in, 0) != cudaSuccess)
         return CHY_ERR_CUDA;
+    for (int i = 0; i < nb; i++)
+        if (mapped[i] && chy_internal_rim_in(bp.phi[i], mapped[i], c.J, c.K, c.L, ln.stream) != cudaSuccess)
+            return CHY_ERR_CUDA;
     int st = chy_internal_run_batch(ln.plan, bp, nb, ln.stream);
     if (st != CHY_OK) return st;
     // the mode solve's error word, read back with the batch into the slot's own

@@ -429,6 +429,14 @@ def test_host_copies_read_and_write_only_their_cells(chylib, prec):
     host = plan.solve(dirty, phi0.copy(order="F"))
     assert np.array_equal(host, ref)
     assert np.array_equal(host[:, K + 1, :], phi0[:, K + 1, :]) and np.array_equal(host[J + 1, 0, :], phi0[J + 1, 0, :])
+    # pinned host arrays: the untouched cells are read through the array's
+    # device mapping by a kernel instead of being copied
+    pr = chylib.pinned_fortran(dirty.shape)
+    pr[...] = dirty
+    pp = chylib.pinned_fortran(dirty.shape)
+    pp[...] = phi0
+    plan.solve(pr, pp)
+    assert np.array_equal(np.asarray(pp), ref)
     srv = chylib.Server(prec, hbm_budget=4 << 30, max_batch=2)
     try:
         a = chylib.pinned_fortran(dirty.shape)
