@@ -140,6 +140,30 @@ __device__ __forceinline__ void load_fft_tables(const FftDev &f, const FftSmem &
     for (int i = threadIdx.x; i < f.ncompact; i += blockDim.x) s.on[i] = f.onc[i];
 }
 
+// Bytes of one direction's tables as bulk_fft_tables moves them.
+__device__ __forceinline__ uint32_t fft_bulk_bytes(const FftDev &f)
+{
+    return (uint32_t)(f.ncompact * 48 + f.nh * 16 + f.n * 4 + ((f.ncompact + 15) & ~15));
+}
+
+// One direction's tables as four bulk copies (one per table, issued by
+// lane 0 of warps w0 .. w0+3) counted on bar: every source and destination
+// starts on a 16-byte boundary and the flag bytes are padded to 16 (the
+// packed table image leaves 256-byte gaps).  A bulk copy holds its issuing
+// thread while the copy engine takes it in, so no warp issues more than one.
+__device__ __forceinline__ void bulk_fft_tables(const FftDev &f, const FftSmem &s, uint64_t *bar, int w0)
+{
+    const int w = (int)(threadIdx.x >> 5) - w0;
+    if ((threadIdx.x & 31) != 0 || w < 0 || w > 3) return;
+    const void *src = w == 0 ? (const void *)f.twc : w == 1 ? (const void *)f.rt : w == 2 ? (const void *)f.perm : (const void *)f.onc;
+    void *dst = w == 0 ? (void *)s.tw : w == 1 ? (void *)s.rt : w == 2 ? (void *)s.perm : (void *)s.on;
+    const uint32_t bytes = w == 0 ? f.ncompact * 48 : w == 1 ? f.nh * 16 : w == 2 ? f.n * 4 : (f.ncompact + 15) & ~15;
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     sm32(dst)),
+                 "l"(src), "r"(bytes), "r"(sm32(bar))
+                 : "memory");
+}
+
 template <int L>
 __host__ __device__ constexpr size_t fft_table_bytes()
 {
@@ -340,16 +364,32 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
         __syncthreads();
         if (threadIdx.x == 0) {
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm32(tbar)),
-                         "r"((uint32_t)(L * T::RS * 8)));
+                         "r"((uint32_t)(L * T::RS * 8) + fft_bulk_bytes(t.fwd) + 20u * (L / 4) * 8u));
             for (int l0 = 0; l0 < L; l0 += 256) tma_load_3d(A0 + (size_t)l0 * T::RS, &maps.m[b], j0, k + 1, l0, tbar);
         }
-    }
-
-    // tables and the tile's samples: every copy in flight at once
-    load_fft_tables(t.fwd, fs);
-    for (int i = threadIdx.x; i < 20 * (L / 4); i += blockDim.x) {
-        const int m = i / (L / 4), l = i % (L / 4);
-        cp_async8(mtab + i, m < 10 ? t.cosm + (size_t)m * L + l : t.sinm + (size_t)(m - 10) * L + l, 8);
+        // the tables on the same barrier: the transform's by lane 0 of warps
+        // 1-4, the 20 moment rows (L/4 cos or sin values each) by lanes 0-3
+        // of warps 5-7, 0 and 1, one row per thread
+        bulk_fft_tables(t.fwd, fs, tbar, 1);
+        {
+            const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+            const int m = ln < 4 ? (w >= 5 ? (w - 5) * 4 + ln : 12 + w * 4 + ln) : 99;
+            if (m < 20) {
+                const double *src = m < 10 ? t.cosm + (size_t)m * L : t.sinm + (size_t)(m - 10) * L;
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        sm32(mtab + (size_t)m * (L / 4))),
+                    "l"(src), "r"((uint32_t)(L / 4) * 8u), "r"(sm32(tbar))
+                    : "memory");
+            }
+        }
+    } else {
+        // tables and the tile's samples: every copy in flight at once
+        load_fft_tables(t.fwd, fs);
+        for (int i = threadIdx.x; i < 20 * (L / 4); i += blockDim.x) {
+            const int m = i / (L / 4), l = i % (L / 4);
+            cp_async8(mtab + i, m < 10 ? t.cosm + (size_t)m * L + l : t.sinm + (size_t)(m - 10) * L + l, 8);
+        }
     }
     if (vec16 == 2) {
         // copies issued above
@@ -687,14 +727,17 @@ __global__ void __launch_bounds__(256) k_inverse(DevTables t, BatchPtrs bp, Work
         if (threadIdx.x == 0) {
             constexpr int B = n < 256 ? n : 256;
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm32(tbar)),
-                         "r"((uint32_t)(2 * n * RS * 8)));
+                         "r"((uint32_t)(2 * n * RS * 8) + fft_bulk_bytes(t.inv)));
             for (int z0 = 0; z0 < n; z0 += B) {
                 tma_load_3d(A + (size_t)z0 * RS, &xmap, j0, k, b * L + z0, tbar);
                 tma_load_3d(A + (size_t)(I0 + z0) * RS, &xmap, j0, k, b * L + n + z0, tbar);
             }
         }
+        // the tables on the same barrier (lane 0 of warps 1-4)
+        bulk_fft_tables(t.inv, fs, tbar, 1);
+    } else {
+        load_fft_tables(t.inv, fs);
     }
-    load_fft_tables(t.inv, fs);
     if (xmode == 2) {
         // copies issued above
     } else if (xmode == 1) {
