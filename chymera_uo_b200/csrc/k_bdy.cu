@@ -19,16 +19,16 @@
 
 namespace chy {
 
-// Grid: (nsub, 1, ceil(batch / kSubBatch)).  The ring-table slice of a
-// sub-chunk is loaded once and serves up to kSubBatch solves; when the 2*ncol
-// column sums of one solve fill at most half the block, two solves are summed
-// side by side.  Every column sum keeps its order, whatever the pairing.
+// Grid: (nsub, 1, ceil(batch / kSubBatch)), four threads per column.  The
+// ring-table slice of a sub-chunk is loaded once and serves up to kSubBatch
+// solves, two solves per pass.  Every column sum keeps its order, whatever
+// the pairing.
 constexpr int kSubBatch = 8;
 constexpr int kSubThreads = 512;
 __global__ void __launch_bounds__(kSubThreads) k_bdy_sub(DevTables t, Work w, int nb, int spp)
 {
     extern __shared__ double smem[];
-    const int RL = t.srow, NT_ = t.ntrm, per = 2 * t.ncol;
+    const int RL = t.srow, NT_ = t.ntrm;
     double *s_row = smem;                                      // [ns][RL]: TERM, r^-(2l+1), DV
     double *s_mom = smem + kSubChunk * RL;                     // [spp][ns][21]
     int *s_ring = reinterpret_cast<int *>(s_mom + (size_t)spp * kSubChunk * 21);   // [ns] ring index
@@ -50,36 +50,60 @@ __global__ void __launch_bounds__(kSubThreads) k_bdy_sub(DevTables t, Work w, in
             s_mom[((size_t)sl * kSubChunk + r) * 21 + q] = s_row[r * RL + NT_ + 11] * mom[(size_t)q * t.nring + s_ring[r]];
         }
         __syncthreads();
-        for (int task = threadIdx.x; task < nsl * per; task += blockDim.x) {
-            const int sl = task / per, cc = task % per;
-            const int col = cc % t.ncol, out = cc / t.ncol;
-            const int term = t.col_term[col], m = t.col_m[col], l = t.col_l[col];
-            const int mq = t.col_part[col] == 0 ? m : 10 + m;
-            const double *sm = s_mom + (size_t)sl * kSubChunk * 21;
-            // four partial sums (rings 4i .. 4i+3 into a0 .. a3, a remainder
-            // into a0), then (a0 + a1) + (a2 + a3): a fixed order with a
-            // quarter of the dependent chain
-            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-            int r = 0;
-            if (!out) {
-                for (; r + 4 <= ns; r += 4) {
-                    a0 = a0 + s_row[r * RL + term] * sm[r * 21 + mq];
-                    a1 = a1 + s_row[(r + 1) * RL + term] * sm[(r + 1) * 21 + mq];
-                    a2 = a2 + s_row[(r + 2) * RL + term] * sm[(r + 2) * 21 + mq];
-                    a3 = a3 + s_row[(r + 3) * RL + term] * sm[(r + 3) * 21 + mq];
-                }
-                for (; r < ns; ++r) a0 = a0 + s_row[r * RL + term] * sm[r * 21 + mq];
-            } else {
-                for (; r + 4 <= ns; r += 4) {
-                    a0 = a0 + (s_row[r * RL + term] * sm[r * 21 + mq]) * s_row[r * RL + NT_ + l];
-                    a1 = a1 + (s_row[(r + 1) * RL + term] * sm[(r + 1) * 21 + mq]) * s_row[(r + 1) * RL + NT_ + l];
-                    a2 = a2 + (s_row[(r + 2) * RL + term] * sm[(r + 2) * 21 + mq]) * s_row[(r + 2) * RL + NT_ + l];
-                    a3 = a3 + (s_row[(r + 3) * RL + term] * sm[(r + 3) * 21 + mq]) * s_row[(r + 3) * RL + NT_ + l];
-                }
-                for (; r < ns; ++r) a0 = a0 + (s_row[r * RL + term] * sm[r * 21 + mq]) * s_row[r * RL + NT_ + l];
+        // Column col's inside and outside sums of these solves, each as four
+        // partial sums (rings 4i .. 4i+3 into a0 .. a3, a remainder into a0)
+        // added as (a0 + a1) + (a2 + a3): a fixed order with a quarter of the
+        // dependent chain.  Lane 4 c + i of a warp holds partial sum a_i of
+        // its column for both sums and both solves, so a ring's TERM and
+        // r^-(2l+1) are read once for four accumulations and the product
+        // TERM * DV * MRING once for the inside and the outside sum.
+        {
+            const int col = threadIdx.x >> 2, ph = threadIdx.x & 3;
+            const bool live = col < t.ncol;
+            int term = 0, l = 0, mq = 0;
+            if (live) {
+                term = t.col_term[col];
+                l = t.col_l[col];
+                mq = t.col_part[col] == 0 ? t.col_m[col] : 10 + t.col_m[col];
             }
-            const double acc = (a0 + a1) + (a2 + a3);
-            w.sub[(size_t)(b + sl) * w.ssub + (size_t)sc * 2 * t.ncol + (size_t)out * t.ncol + col] = acc;
+            const double *sm0 = s_mom, *sm1 = s_mom + (size_t)kSubChunk * 21;
+            double ai0 = 0.0, ao0 = 0.0, ai1 = 0.0, ao1 = 0.0;
+            auto ring = [&](int r) {
+                const double tt = s_row[r * RL + term], qh = s_row[r * RL + NT_ + l];
+                const double p0 = tt * sm0[r * 21 + mq];
+                ai0 = ai0 + p0;
+                ao0 = ao0 + p0 * qh;
+                if (nsl > 1) {
+                    const double p1 = tt * sm1[r * 21 + mq];
+                    ai1 = ai1 + p1;
+                    ao1 = ao1 + p1 * qh;
+                }
+            };
+            const int q4 = ns & ~3;
+            if (live) {
+                for (int r = ph; r < q4; r += 4) ring(r);
+                if (ph == 0)
+                    for (int r = q4; r < ns; ++r) ring(r);
+            }
+            // (a0 + a1) + (a2 + a3); IEEE addition commutes, so every lane of
+            // the four ends with the same bits
+            auto tree = [&](double v) {
+                v = v + __shfl_xor_sync(0xffffffffu, v, 1);
+                return v + __shfl_xor_sync(0xffffffffu, v, 2);
+            };
+            ai0 = tree(ai0);
+            ao0 = tree(ao0);
+            ai1 = tree(ai1);
+            ao1 = tree(ao1);
+            if (live && ph == 0) {
+                double *sub = w.sub + (size_t)b * w.ssub + (size_t)sc * 2 * t.ncol + col;
+                sub[0] = ai0;
+                sub[t.ncol] = ao0;
+                if (nsl > 1) {
+                    sub[w.ssub] = ai1;
+                    sub[w.ssub + t.ncol] = ao1;
+                }
+            }
         }
     }
 }
@@ -136,10 +160,11 @@ __global__ void __launch_bounds__(256) k_bdy_scan(DevTables t, Work w)
 
 cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStream_t s)
 {
-    // two solves per pass when there are two and a solve's column sums fill
-    // at most half the block
-    const int per = 2 * t.ncol, spp = (nb >= 2 && 2 * per <= kSubThreads) ? 2 : 1;
-    const int threads = spp == 2 ? ((2 * per + 31) / 32) * 32 : 256;
+    // four lanes per column (one per partial sum), two solves per pass
+    // when there are two
+    if (4 * t.ncol > kSubThreads) return cudaErrorInvalidConfiguration;
+    const int spp = nb >= 2 ? 2 : 1;
+    const int threads = ((4 * t.ncol + 31) / 32) * 32;
     const size_t sm = (size_t)kSubChunk * (t.srow + 21 * spp) * sizeof(double) + (size_t)kSubChunk * sizeof(int);
     cudaError_t e = ensure_smem((const void *)k_bdy_sub, sm);
     if (e != cudaSuccess) return e;
