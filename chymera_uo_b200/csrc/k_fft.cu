@@ -420,25 +420,27 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
     // azimuthal moments of each ring (pot/boundary.f:527-538), before DV, using
     // psi -> pi - psi, pi + psi, 2 pi - psi to fold the sum to a quarter period
     {
-        // With 16 threads per column, lanes alternate between a warp's two
-        // columns (so that a half-warp reads 8 rows of 2 columns: no bank
-        // conflict at the even row stride); otherwise a column's threads are
-        // consecutive lanes.  SH is the lane distance between a column's
-        // threads g and g+1.
-        constexpr int SH = T::TPC == 16 ? 2 : 1;
-        const int c = SH == 2 ? 2 * (threadIdx.x >> 5) + (threadIdx.x & 1) : threadIdx.x / T::TPC;
-        const int g = SH == 2 ? (threadIdx.x & 31) >> 1 : threadIdx.x % T::TPC;
+        // The first half of the block forms the cosine sums (q = 0..10), the
+        // second half the sine sums (q = 11..20), of every column of the tile
+        // at once, TPM = 128/TC threads per column.  With 8 threads per
+        // column, lanes alternate between a half-warp's two columns (so that
+        // a half-warp reads 8 rows of 2 columns: no bank conflict at the even
+        // row stride); otherwise a column's threads are consecutive lanes.
+        // SH is the lane distance between a column's threads g and g+1.
+        // A warp's table reads serve 4 (TC = 16) columns at a time.
+        constexpr int TPM = 128 / T::TC;
+        constexpr int SH = TPM == 8 ? 2 : 1;
+        const int th = threadIdx.x & 127;
+        const int c = SH == 2 ? 2 * (th >> 4) + (th & 1) : th / TPM;
+        const int g = SH == 2 ? (th & 15) >> 1 : th % TPM;
         constexpr int Q = L / 4;
-        // The cosine sums (q = 0..10) and the sine sums (q = 11..20) are
-        // formed in two passes over the samples, so that only one set of
-        // accumulators is live at a time.  Butterfly reduce-scatter over the
-        // column's TPC lanes (the pass's sums padded to NS): at each level a
-        // lane keeps half of its live sums and adds the partner's copy of
-        // them, so lane g ends with the column totals of sums base(g) ..
-        // base(g) + NS/TPC - 1.  Every total is the same pairwise tree over
-        // the TPC lanes whichever lane ends with it, so the pass split
-        // changes no bit.
-        constexpr int NS = T::TPC > 16 ? T::TPC : 16;
+        // Butterfly reduce-scatter over the column's TPM lanes (the half's
+        // sums padded to NS): at each level a lane keeps half of its live
+        // sums and adds the partner's copy of them, so lane g ends with the
+        // column totals of sums base(g) .. base(g) + NS/TPM - 1.  Every total
+        // is the same pairwise tree over the TPM lanes whichever lane ends
+        // with it.
+        constexpr int NS = TPM > 16 ? TPM : 16;
         const int j = j0 + c;
         double *mom = w.mom + (size_t)b * w.smom + (size_t)k * t.M + j;
         auto pass = [&](auto sine) {
@@ -448,8 +450,8 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
 #pragma unroll
             for (int q = 0; q < NS; ++q) a[q] = 0.0;
 #pragma unroll
-            for (int il = 0; il < Q / T::TPC; ++il) {
-                const int l = g + il * T::TPC;
+            for (int il = 0; il < Q / TPM; ++il) {
+                const int l = g + il * TPM;
                 const double r1 = A[l * T::RS + c], r2 = A[(L / 2 - 1 - l) * T::RS + c];
                 const double r3 = A[(L / 2 + l) * T::RS + c], r4 = A[(L - 1 - l) * T::RS + c];
                 if constexpr (!S) {
@@ -468,8 +470,8 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
             }
             int base = 0;
 #pragma unroll
-            for (int lev = 0; (T::TPC >> (lev + 1)) >= 1; ++lev) {
-                const int o = T::TPC >> (lev + 1), W = NS >> lev;
+            for (int lev = 0; (TPM >> (lev + 1)) >= 1; ++lev) {
+                const int o = TPM >> (lev + 1), W = NS >> lev;
                 const bool up = (g & o) != 0;
 #pragma unroll
                 for (int i = 0; i < W / 2; ++i) {
@@ -481,12 +483,12 @@ __global__ void __launch_bounds__(256) k_forward(DevTables t, BatchPtrs bp, Work
             }
             if (j < t.M) {
 #pragma unroll
-                for (int i = 0; i < NS / T::TPC; ++i)
+                for (int i = 0; i < NS / TPM; ++i)
                     if (base + i < NQ) mom[(size_t)(Q0 + base + i) * t.nring] = a[i];
             }
         };
-        pass(std::integral_constant<bool, false>{});
-        pass(std::integral_constant<bool, true>{});
+        if (threadIdx.x < 128) pass(std::integral_constant<bool, false>{});
+        else pass(std::integral_constant<bool, true>{});
     }
     __syncthreads();
 
