@@ -108,54 +108,48 @@ __global__ void __launch_bounds__(kSubThreads) k_bdy_sub(DevTables t, Work w, in
     }
 }
 
-// Grid: (2*ncol, 1, batch), 256 threads: one CTA scans one column.
+// Grid: (ceil(2*ncol / 32), 1, batch), 256 threads: lane i of every warp
+// takes column 32 blockIdx.x + i of the [2][ncol] row (inside sums, then
+// outside sums), so each row is read and written in one coalesced piece;
+// warp s takes the s-th of eight consecutive runs of sub-chunks in scan order.
 // scan[i][0][col] = sum of inside sums of sub-chunks < i (prefix from the
 // innermost ring); scan[i][1][col] = sum of outside sums of sub-chunks >= i
-// (suffix from the outermost ring).  Each thread owns a contiguous run of
-// sub-chunks; runs are combined by a fixed-shape block scan, so the result is
-// bit-reproducible.
+// (suffix from the outermost ring).  Each run is summed in order, the run
+// totals are added in order, and every prefix is that base plus the run's
+// running sum: a fixed order, so the result is bit-reproducible.
 __global__ void __launch_bounds__(256) k_bdy_scan(DevTables t, Work w)
 {
-    __shared__ double warp_tot[8];
-    const int cc = blockIdx.x, b = blockIdx.z;
-    const int col = cc % t.ncol, out = cc / t.ncol;
+    __shared__ double run_tot[8][32];
+    const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5, b = blockIdx.z;
+    const int cc = blockIdx.x * 32 + lane, ld = 2 * t.ncol;
+    const bool live = cc < ld, out = cc >= t.ncol;
     const double *__restrict__ sub = w.sub + (size_t)b * w.ssub;
     double *__restrict__ scan = w.scan + (size_t)b * w.sscan;
-    const size_t ld = (size_t)2 * t.ncol, off = (size_t)out * t.ncol + col;
-    const int ns = t.nsub, per = (ns + 255) / 256;
-    const int lo = threadIdx.x * per, hi = min(lo + per, ns);
+    const int ns = t.nsub, per = (ns + 7) / 8;
+    const int lo = min(seg * per, ns), hi = min(lo + per, ns);
     // position p in scan order -> sub-chunk index
     auto idx = [&](int p) { return out ? ns - 1 - p : p; };
     double local = 0.0;
-    for (int p = lo; p < hi; ++p) local = local + sub[(size_t)idx(p) * ld + off];
-    // exclusive block scan of the per-thread totals
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double incl = local;
-    for (int o = 1; o < 32; o <<= 1) {
-        const double v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl = incl + v;
-    }
-    if (lane == 31) warp_tot[wid] = incl;
+    if (live)
+        for (int p = lo; p < hi; ++p) local = local + sub[(size_t)idx(p) * ld + cc];
+    run_tot[seg][lane] = local;
     __syncthreads();
     double base = 0.0;
-    for (int i = 0; i < wid; ++i) base = base + warp_tot[i];
-    double run = base + (incl - local);
+    for (int i = 0; i < seg; ++i) base = base + run_tot[i][lane];
+    if (!live) return;
+    double run = base;
     for (int p = lo; p < hi; ++p) {
         const int i = idx(p);
-        const double v = sub[(size_t)i * ld + off];
+        const double v = sub[(size_t)i * ld + cc];
         if (!out) {
-            scan[(size_t)i * ld + off] = run;
+            scan[(size_t)i * ld + cc] = run;
             run = run + v;
         } else {
             run = run + v;
-            scan[(size_t)i * ld + off] = run;
+            scan[(size_t)i * ld + cc] = run;
         }
     }
-    if (threadIdx.x == 255) {
-        double tot = 0.0;
-        for (int i = 0; i < 8; ++i) tot = tot + warp_tot[i];
-        scan[(size_t)ns * ld + off] = out ? 0.0 : tot;
-    }
+    if (seg == 7) scan[(size_t)ns * ld + cc] = out ? 0.0 : run;   // the inside total
 }
 
 cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStream_t s)
@@ -171,7 +165,7 @@ cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStrea
     k_bdy_sub<<<dim3(t.nsub, 1, (nb + kSubBatch - 1) / kSubBatch), threads, sm, s>>>(t, w, nb, spp);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_bdy_scan<<<dim3(2 * t.ncol, 1, nb), 256, 0, s>>>(t, w);
+    k_bdy_scan<<<dim3((2 * t.ncol + 31) / 32, 1, nb), 256, 0, s>>>(t, w);
     return cudaGetLastError();
 }
 
