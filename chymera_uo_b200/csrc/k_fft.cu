@@ -569,14 +569,22 @@ __global__ void __launch_bounds__(256) k_bdy_synth(DevTables t, Work w)
         cq[c][q] = -t.grav * (q == 0 ? s : 2.0 * s);
     }
     __syncthreads();
+    // one azimuth l per thread: its 21 basis values are read once and serve
+    // the block's kPts boundary points
     double *X = w.X + (size_t)b * w.sX;
-    for (int i = threadIdx.x; i < kPts * L; i += blockDim.x) {
-        const int c = i / L, l = i % L, q = q0 + c;
-        if (q < t.njk) {
-            double v = 0.0;
+    for (int l = threadIdx.x; l < L; l += blockDim.x) {
+        double f[21];
 #pragma unroll
-            for (int p = 0; p < 21; ++p) v = __fma_rn(cq[c][p], __ldg(t.fbasis + (size_t)p * L + l), v);
-            X[((size_t)l * t.K + t.jk_k[q]) * t.J + t.jk_j[q]] = v;
+        for (int p = 0; p < 21; ++p) f[p] = __ldg(t.fbasis + (size_t)p * L + l);
+#pragma unroll 2
+        for (int c = 0; c < kPts; ++c) {
+            const int q = q0 + c;
+            if (q < t.njk) {
+                double v = 0.0;
+#pragma unroll
+                for (int p = 0; p < 21; ++p) v = __fma_rn(cq[c][p], f[p], v);
+                X[((size_t)l * t.K + t.jk_k[q]) * t.J + t.jk_j[q]] = v;
+            }
         }
     }
 }
