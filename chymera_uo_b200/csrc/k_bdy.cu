@@ -108,48 +108,66 @@ __global__ void __launch_bounds__(kSubThreads) k_bdy_sub(DevTables t, Work w, in
     }
 }
 
-// Grid: (ceil(2*ncol / 32), 1, batch), 256 threads: lane i of every warp
+// Grid: (ceil(2*ncol / 32), 1, batch), 512 threads: lane i of every warp
 // takes column 32 blockIdx.x + i of the [2][ncol] row (inside sums, then
 // outside sums), so each row is read and written in one coalesced piece;
-// warp s takes the s-th of eight consecutive runs of sub-chunks in scan order.
+// warp s takes the s-th of kScanRuns consecutive runs of sub-chunks in scan
+// order.
 // scan[i][0][col] = sum of inside sums of sub-chunks < i (prefix from the
 // innermost ring); scan[i][1][col] = sum of outside sums of sub-chunks >= i
 // (suffix from the outermost ring).  Each run is summed in order, the run
 // totals are added in order, and every prefix is that base plus the run's
 // running sum: a fixed order, so the result is bit-reproducible.
-__global__ void __launch_bounds__(256) k_bdy_scan(DevTables t, Work w)
+constexpr int kScanRuns = 16;
+__global__ void __launch_bounds__(32 * kScanRuns) k_bdy_scan(DevTables t, Work w)
 {
-    __shared__ double run_tot[8][32];
+    __shared__ double run_tot[kScanRuns][32];
     const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5, b = blockIdx.z;
     const int cc = blockIdx.x * 32 + lane, ld = 2 * t.ncol;
     const bool live = cc < ld, out = cc >= t.ncol;
     const double *__restrict__ sub = w.sub + (size_t)b * w.ssub;
     double *__restrict__ scan = w.scan + (size_t)b * w.sscan;
-    const int ns = t.nsub, per = (ns + 7) / 8;
+    const int ns = t.nsub, per = (ns + kScanRuns - 1) / kScanRuns;
     const int lo = min(seg * per, ns), hi = min(lo + per, ns);
     // position p in scan order -> sub-chunk index
     auto idx = [&](int p) { return out ? ns - 1 - p : p; };
+    // loads go eight at a time, so that their latencies overlap; the sums
+    // stay in order
+    constexpr int kU = 8;
     double local = 0.0;
     if (live)
-        for (int p = lo; p < hi; ++p) local = local + sub[(size_t)idx(p) * ld + cc];
+        for (int p0 = lo; p0 < hi; p0 += kU) {
+            double v[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) v[u] = p0 + u < hi ? sub[(size_t)idx(p0 + u) * ld + cc] : 0.0;
+#pragma unroll
+            for (int u = 0; u < kU; ++u)
+                if (p0 + u < hi) local = local + v[u];
+        }
     run_tot[seg][lane] = local;
     __syncthreads();
     double base = 0.0;
     for (int i = 0; i < seg; ++i) base = base + run_tot[i][lane];
     if (!live) return;
     double run = base;
-    for (int p = lo; p < hi; ++p) {
-        const int i = idx(p);
-        const double v = sub[(size_t)i * ld + cc];
-        if (!out) {
-            scan[(size_t)i * ld + cc] = run;
-            run = run + v;
-        } else {
-            run = run + v;
-            scan[(size_t)i * ld + cc] = run;
+    for (int p0 = lo; p0 < hi; p0 += kU) {
+        double v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) v[u] = p0 + u < hi ? sub[(size_t)idx(p0 + u) * ld + cc] : 0.0;
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            if (p0 + u >= hi) break;
+            const size_t at = (size_t)idx(p0 + u) * ld + cc;
+            if (!out) {
+                scan[at] = run;
+                run = run + v[u];
+            } else {
+                run = run + v[u];
+                scan[at] = run;
+            }
         }
     }
-    if (seg == 7) scan[(size_t)ns * ld + cc] = out ? 0.0 : run;   // the inside total
+    if (seg == kScanRuns - 1) scan[(size_t)ns * ld + cc] = out ? 0.0 : run;   // the inside total
 }
 
 cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStream_t s)
@@ -165,7 +183,7 @@ cudaError_t launch_bdy_sums(const DevTables &t, const Work &w, int nb, cudaStrea
     k_bdy_sub<<<dim3(t.nsub, 1, (nb + kSubBatch - 1) / kSubBatch), threads, sm, s>>>(t, w, nb, spp);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_bdy_scan<<<dim3((2 * t.ncol + 31) / 32, 1, nb), 256, 0, s>>>(t, w);
+    k_bdy_scan<<<dim3((2 * t.ncol + 31) / 32, 1, nb), 32 * kScanRuns, 0, s>>>(t, w);
     return cudaGetLastError();
 }
 
