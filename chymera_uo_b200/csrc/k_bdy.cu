@@ -8,8 +8,9 @@
 // spherical radius, MASSIN(JK) is a prefix sum and MASSOUT(JK) a suffix sum
 // of the same sequence, cut at the number of rings inside RBDY(JK).  The
 // sorted sequence is split into sub-chunks that never straddle a cut; one CTA
-// sums each sub-chunk, one thread per column scans the sub-chunk sums.  Every
-// sum has a fixed order, so results are bit-reproducible alone or in a batch.
+// sums each sub-chunk, and each column's sub-chunk sums are scanned in
+// in-order runs.  Every sum has a fixed order, so results are bit-reproducible
+// alone or in a batch.
 // The outside sums are accumulated from the outermost ring inward, so the
 // huge r^-(2l+1) factors of inner rings never enter a difference.
 //
