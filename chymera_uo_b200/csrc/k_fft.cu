@@ -1030,6 +1030,8 @@ static cudaError_t forward_l(const DevTables &t, const BatchPtrs &bp, const Work
         }
         if (ok) vec16 = 2;
     }
+    // 256 threads: the table copies, the moment halves and the compile-time
+    // trip counts of k_forward assume eight warps
     k_forward<L><<<dim3((t.M + T::TC - 1) / T::TC, t.NZ, nb), 256, sm, s>>>(t, bp, w, vec16, maps);
     return cudaGetLastError();
 }
@@ -1057,6 +1059,8 @@ static cudaError_t inverse_l(const DevTables &t, const BatchPtrs &bp, const Work
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
             xmode = 2;
     }
+    // 256 threads: the table copies and the compile-time trip counts of
+    // k_inverse assume eight warps
     k_inverse<L><<<dim3((t.J + T::TC - 1) / T::TC, t.K, nb), 256, sm, s>>>(t, bp, w, x, xmode, xmap);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     *launches = 2;
