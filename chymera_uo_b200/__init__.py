@@ -183,6 +183,8 @@ def lib():
         L.chy_plan_star_potential.restype = i
         L.chy_source.argtypes = [vp, C.POINTER(ChySourceArgs), vp]
         L.chy_source.restype = i
+        L.chy_source_binary.argtypes = [vp, C.POINTER(ChySourceArgs), C.POINTER(ChyBinary), C.c_double, vp, vp]
+        L.chy_source_binary.restype = i
         _lib = L
     return _lib
 
@@ -328,15 +330,20 @@ class Plan:
         _check(lib().chy_plan_star_potential(self._p, out.ctypes.data, CHY_PTR_HOST, stream or 0))
         return out
 
-    def source(self, rho, phi, omega, p, s, t, a, delt: float, jmin: int = 2, stream=None):
+    def source(self, rho, phi, omega, p, s, t, a, delt: float, jmin: int = 2, stream=None, binary=None):
         """SOURCE's potential, pressure and rotation terms (radhydro/source.f:45-81)
         on CUDA tensors (column-major): s, t, a updated in place.  omega, p,
         s, t, a are (JMAX+2, KMAX+2, LMAX) of the hydro grid; rho, phi the
-        plan's grid."""
+        plan's grid.
+
+        binary: None (a BINARY = 0 build), or a dict with ``u`` (U, a hydro
+        array), ``mass_star`` and optionally ``mass_bin`` (1) and ``a_bin``
+        (100) for the BINARY build's terms (``chy_source_binary``)."""
         hshape = tuple(omega.shape)
         for x in (rho, phi):
             self._validate(x, True)
-        for x in (omega, p, s, t, a):
+        hydro = (omega, p, s, t, a) + ((binary["u"],) if binary is not None else ())
+        for x in hydro:
             if not _is_cuda_tensor(x) or tuple(x.shape) != hshape or str(x.dtype) != "torch.float64":
                 raise ValueError(f"hydro arrays must be float64 CUDA tensors of one shape {hshape}")
             if x.stride() != (1, hshape[0], hshape[0] * hshape[1]):
@@ -345,7 +352,12 @@ class Plan:
             raise ValueError("hydro and potential grids share LMAX")
         args = ChySourceArgs(hshape[0] - 2, hshape[1] - 2, jmin, delt, rho.data_ptr(), phi.data_ptr(),
                              omega.data_ptr(), p.data_ptr(), s.data_ptr(), t.data_ptr(), a.data_ptr())
-        _check(lib().chy_source(self._p, C.byref(args), self._stream(stream)))
+        if binary is None:
+            _check(lib().chy_source(self._p, C.byref(args), self._stream(stream)))
+            return
+        b = ChyBinary(float(binary.get("mass_bin", 1.0)), float(binary.get("a_bin", 100.0)))
+        _check(lib().chy_source_binary(self._p, C.byref(args), C.byref(b), float(binary["mass_star"]),
+                                       binary["u"].data_ptr(), self._stream(stream)))
 
     def set_profiling(self, on: bool):
         _check(lib().chy_plan_set_profiling(self._p, int(on)))

@@ -431,16 +431,19 @@ int chy_plan_star_potential(chy_plan *p, double *starphi, int ptr_kind, void *st
     return CHY_OK;
 }
 
-int chy_source(chy_plan *p, const chy_source_args *a, void *stream)
+// chy_source and chy_source_binary: SOURCE's loop nest with the BINARY
+// build's terms when q.binary is set (the caller fills q's BINARY fields).
+static int run_source(chy_plan *p, const chy_source_args *a, SourceDev &q, void *stream)
 {
     if (!p || !a) return fail(CHY_ERR_ARG, "null plan or arguments");
     if (!a->rho || !a->phi || !a->omega || !a->p || !a->s || !a->t || !a->a)
         return fail(CHY_ERR_ARG, "null array");
+    const int dst = check_device(p);
+    if (dst != CHY_OK) return dst;
     const HostPlan &hp = p->hp;
     if (a->jmax < 1 || a->kmax < 1 || a->jmax > hp.J || a->kmax > hp.K)
         return fail(CHY_ERR_DIMS, "hydro JMAX/KMAX must be in 1..the plan's JMAX/KMAX");
     if (a->jmin < 1) return fail(CHY_ERR_ARG, "JMIN must be >= 1");
-    SourceDev q{};
     q.J2h = a->jmax + 2;
     q.K2h = a->kmax + 2;
     q.J2p = hp.J + 2;
@@ -465,9 +468,30 @@ int chy_source(chy_plan *p, const chy_source_args *a, void *stream)
     q.R = p->t.r;
     q.rho = a->rho; q.phi = a->phi; q.omega = a->omega; q.p = a->p;
     q.S = a->s; q.T = a->t; q.A = a->a;
+    q.rhf = p->t.rhf;
     CHY_CUDA(launch_source(q, (cudaStream_t)stream));
     p->launches += 1;
     return CHY_OK;
+}
+
+int chy_source(chy_plan *p, const chy_source_args *a, void *stream)
+{
+    SourceDev q{};
+    return run_source(p, a, q, stream);
+}
+
+int chy_source_binary(chy_plan *p, const chy_source_args *a, const chy_binary *b, double mass_star, const double *u,
+                      void *stream)
+{
+    if (!b || !u) return fail(CHY_ERR_ARG, "null binary parameters or U");
+    if (!(b->a_bin > 0.0)) return fail(CHY_ERR_ARG, "binary separation must be positive");
+    SourceDev q{};
+    q.binary = 1;
+    // getBinaryPosition (radhydro/ExternalRoutines.f:101-102), as set_binary_orbit
+    const double mu = b->mass_bin + mass_star;
+    q.omega_bin = std::sqrt((mu) / (b->a_bin * b->a_bin * b->a_bin));
+    q.u = u;
+    return run_source(p, a, q, stream);
 }
 
 long long chy_plan_device_bytes(const chy_plan *p)

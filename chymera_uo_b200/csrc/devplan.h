@@ -128,6 +128,10 @@ struct SourceDev {
     const double *R;     // R(POT3JMAX+2)
     const double *rho, *phi, *omega, *p;
     double *S, *T, *A;
+    // BINARY build's terms (binary != 0): OMEGABIN, RHF(POT3JMAX+2), U
+    int binary;
+    double omega_bin;
+    const double *rhf, *u;
 };
 
 // Raises a kernel's dynamic shared-memory limit on the current device the

@@ -1,6 +1,7 @@
 // k_source.cu -- the potential, pressure and rotation source terms of the
-// momentum equations, SOURCE's first loop nest (radhydro/source.f:45-81,
-// BINARY = 0 builds), on the device, for the PHI a solve has just written.
+// momentum equations, SOURCE's first loop nest (radhydro/source.f:45-81), on
+// the device, for the PHI a solve has just written; with the BINARY build's
+// rotating-frame terms as an option.
 //
 // Per cell of the hydro grid, L = 1..LMAX (periodic), K = 2..KMAX+1:
 //   S(J) += DELT*( R(J)*(RHO_J+RHO_J-1)*(OMEGA_J+OMEGA_J-1)**2 * 1/4 * 1/2
@@ -12,10 +13,14 @@
 // JSTART = MAX(JMIN, 2).  Every product, quotient and sum is rounded on its
 // own, in the reference's order, so the result is the reference's to the bit.
 //
-// HBM-bound: per updated cell 7 reads and 3 writes of 8 bytes.  One CTA per
-// (K, L) row; the neighbour rows K-1 and planes L+-1 that a CTA reads were
-// read by CTAs just before it (blockIdx.x = K runs fastest), so they come
-// from L2 and DRAM traffic stays at the algorithmic 80 bytes per cell.
+// BINARY builds add, in the same statements (source.f:61-62, 76-77),
+//   S += OMEGABIN*OMEGA(J)*RHF(J)*2*RHO(J)*DELT
+//   A -= RHO(J)*OMEGABIN*(U(J+1)+U(J))*DELT*RHF(J)
+// HBM-bound: per updated cell 7 reads and 3 writes of 8 bytes (one more read,
+// U, in BINARY builds).  One CTA per (K, L) row; the neighbour rows K-1 and
+// planes L+-1 that a CTA reads were read by CTAs just before it (blockIdx.x =
+// K runs fastest), so they come from L2 and DRAM traffic stays at the
+// algorithmic 80 bytes per cell.
 #include <cuda_runtime.h>
 
 #include "devplan.h"
@@ -30,6 +35,9 @@ __device__ __forceinline__ double quot(double x, double d, double inv)
     return inv != 0.0 ? __dmul_rn(x, inv) : __ddiv_rn(x, d);
 }
 
+// BIN: the BINARY build's terms (radhydro/source.f:61-62, 76-77), each added
+// after the DELT term of its statement, its product formed left to right.
+template <bool BIN>
 __global__ void __launch_bounds__(256) k_source(SourceDev a)
 {
     const int k = blockIdx.x + 1, l = blockIdx.y;   // 0-based K = 1..KMAX, L
@@ -66,7 +74,16 @@ __global__ void __launch_bounds__(256) k_source(SourceDev a)
             x1 = __dmul_rn(x1, 0.5);
             const double x2 = quot(__dmul_rn(rs, __dsub_rn(f0, fj)), two_dr, a.inv_2dr);
             const double x3 = quot(__dsub_rn(q0, qj), a.dr, a.inv_dr);
-            a.S[h0 + j] = __dadd_rn(s0, __dmul_rn(a.delt, __dsub_rn(__dsub_rn(x1, x2), x3)));
+            double sn = __dadd_rn(s0, __dmul_rn(a.delt, __dsub_rn(__dsub_rn(x1, x2), x3)));
+            if constexpr (BIN) {
+                // + OMEGABIN*OMEGA(J)*RHF(J)*2*RHO(J)*DELT
+                double b = __dmul_rn(a.omega_bin, o0);
+                b = __dmul_rn(b, __ldg(a.rhf + j));
+                b = __dmul_rn(b, 2.0);
+                b = __dmul_rn(b, r0);
+                sn = __dadd_rn(sn, __dmul_rn(b, a.delt));
+            }
+            a.S[h0 + j] = sn;
         }
         // T (radhydro/source.f:67-70)
         const double rz = __dadd_rn(r0, rk);
@@ -76,14 +93,25 @@ __global__ void __launch_bounds__(256) k_source(SourceDev a)
         // A (radhydro/source.f:74-75)
         double z = __dmul_rn(r0, __dsub_rn(fp, fm));
         z = __dsub_rn(__dadd_rn(z, qp), qm);
-        a.A[h0 + j] = __dsub_rn(a0, __ddiv_rn(__dmul_rn(a.delt, z), two_dth));
+        double an = __dsub_rn(a0, __ddiv_rn(__dmul_rn(a.delt, z), two_dth));
+        if constexpr (BIN) {
+            // - RHO(J)*OMEGABIN*(U(J+1)+U(J))*DELT*RHF(J); J+1 <= JMAX+1 is in U
+            double b = __dmul_rn(r0, a.omega_bin);
+            b = __dmul_rn(b, __dadd_rn(__ldg(a.u + h0 + j + 1), __ldg(a.u + h0 + j)));
+            b = __dmul_rn(b, a.delt);
+            an = __dsub_rn(an, __dmul_rn(b, __ldg(a.rhf + j)));
+        }
+        a.A[h0 + j] = an;
     }
 }
 
 cudaError_t launch_source(const SourceDev &a, cudaStream_t s)
 {
     if (a.Kh < 1 || a.L < 1 || a.j0 > a.Jh) return cudaSuccess;
-    k_source<<<dim3(a.Kh, a.L), 256, 0, s>>>(a);
+    if (a.binary)
+        k_source<true><<<dim3(a.Kh, a.L), 256, 0, s>>>(a);
+    else
+        k_source<false><<<dim3(a.Kh, a.L), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

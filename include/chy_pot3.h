@@ -314,6 +314,18 @@ typedef struct chy_source_args {
 /* Device pointers only; S, T, A must not overlap the input arrays.
  * Asynchronous on `stream`. */
 int chy_source(chy_plan *p, const chy_source_args *args, void *stream);
+/* The same loop nest as a BINARY build compiles it (radhydro/source.f:38-40,
+ * 61-62, 76-77): chy_source's updates, then in the same statements
+ *   S += OMEGABIN*OMEGA(J)*RHF(J)*2*RHO(J)*DELT,      J = JSTART+1..JMAX+1,
+ *   A -= RHO(J)*OMEGABIN*(U(J+1)+U(J))*DELT*RHF(J),   J = JSTART..JMAX+1,
+ * each product formed left to right, with OMEGABIN of getBinaryPosition's
+ * circular orbit (radhydro/ExternalRoutines.f:91-105):
+ * SQRT((MASSBIN + MASS_STAR)/ABIN**3), the orbit chy_plan_set_binary's
+ * companion uses.  u is U(JMAX+2, KMAX+2, LMAX), the radial velocity, a
+ * device array that must not overlap S, T, A; mass_star is MASS_STAR (/GAP/).
+ * Bit-identical to the reference's statements, like chy_source. */
+int chy_source_binary(chy_plan *p, const chy_source_args *args, const chy_binary *b, double mass_star,
+                      const double *u, void *stream);
 
 /* Bytes of device work space the plan holds (tables + per-solve scratch). */
 long long chy_plan_device_bytes(const chy_plan *p);

@@ -57,6 +57,8 @@ def lib():
         L.ora_external_pot.argtypes = [vp, d, d, d, d, i, i, dp, dp]
         L.ora_external_pot_binary.argtypes = [vp, d, d, d, d, i, i, i, d, d, dp, dp]
         L.ora_source.argtypes = [i, i, i, i, i, i, d, d, d, d, dp, dp, dp, dp, dp, dp, dp, dp]
+        L.ora_source_binary.argtypes = [i, i, i, i, i, i, d, d, d, d, dp, dp, dp, dp, dp, dp, dp, dp, i, d, d, d,
+                                        dp, dp]
         L.ora_blktri_wsize.argtypes = [i, i]
         _lib = L
     return _lib
@@ -208,10 +210,14 @@ class Oracle:
         return np.array(self.phi, order="F", copy=True)
 
 
-def source(r, rho, phi, omega, p, s, t, a, delt, dr, dz, dtheta, jmin=2):
+def source(r, rho, phi, omega, p, s, t, a, delt, dr, dz, dtheta, jmin=2, binary=None):
     """SOURCE's first loop nest (radhydro/source.f:45-81) on Fortran-ordered
     arrays: omega, p, s, t, a of the hydro grid (JMAX+2, KMAX+2, LMAX); rho,
-    phi of the potential grid.  s, t, a are updated in place."""
+    phi of the potential grid.  s, t, a are updated in place.
+
+    binary: None for a BINARY = 0 build, else a dict with mass_star, mass_bin,
+    a_bin, rhf (RHF of the potential grid) and u (U, hydro grid) for the
+    BINARY build's terms (source.f:38-40, 61-62, 76-77)."""
     j2, k2, lmax = omega.shape
     j2p, k2p, _ = rho.shape
     for x in (rho, phi, omega, p, s, t, a):
@@ -219,8 +225,17 @@ def source(r, rho, phi, omega, p, s, t, a, delt, dr, dz, dtheta, jmin=2):
     for x in (omega, p, s, t, a):
         assert x.shape == (j2, k2, lmax)
     assert phi.shape == rho.shape and r.shape[0] >= j2p
-    lib().ora_source(j2 - 2, k2 - 2, lmax, j2p, k2p, jmin, delt, dr, dz, dtheta, _dp(np.ascontiguousarray(r)),
-                     _dp(rho), _dp(phi), _dp(omega), _dp(p), _dp(s), _dp(t), _dp(a))
+    args = (j2 - 2, k2 - 2, lmax, j2p, k2p, jmin, delt, dr, dz, dtheta, _dp(np.ascontiguousarray(r)),
+            _dp(rho), _dp(phi), _dp(omega), _dp(p), _dp(s), _dp(t), _dp(a))
+    if binary is None:
+        lib().ora_source(*args)
+        return
+    u = binary["u"]
+    rhf = np.ascontiguousarray(binary["rhf"], dtype=np.float64)
+    assert u.dtype == np.float64 and u.flags.f_contiguous and u.shape == (j2, k2, lmax)
+    assert rhf.shape[0] >= j2p
+    lib().ora_source_binary(*args, 1, float(binary["mass_star"]), float(binary["mass_bin"]), float(binary["a_bin"]),
+                            _dp(rhf), _dp(u))
 
 
 def blktri_solve(an, bn, cn, am, bm, cm, y):

@@ -2173,20 +2173,32 @@ void ora_external_pot(ora_ctx *c, double mass_star, double tmassacc, double rpst
 }
 
 /* ------------------------------------------------------------------------ */
-/* SOURCE's first loop nest (radhydro/source.f:45-81, BINARY = 0): the       */
-/* potential, pressure and rotation terms of the S, T, A momenta.            */
+/* SOURCE's first loop nest (radhydro/source.f:45-81): the potential,        */
+/* pressure and rotation terms of the S, T, A momenta, with the BINARY       */
+/* build's terms when binary != 0.                                           */
 /* ------------------------------------------------------------------------ */
-/* Hydro arrays omega, p, s, t, a are (jmax+2, kmax+2, lmax); rho and phi are
- * the potential grid's (j2p, k2p, lmax); r is R(j2p).  Column-major. */
-void ora_source(int jmax, int kmax, int lmax, int j2p, int k2p, int jmin, double delt, double dr, double dz,
-                double dtheta, const double *r, const double *rho, const double *phi, const double *omega,
-                const double *p, double *s, double *t, double *a)
+/* Hydro arrays omega, p, s, t, a, u are (jmax+2, kmax+2, lmax); rho and phi
+ * are the potential grid's (j2p, k2p, lmax); r and rhf are R(j2p), RHF(j2p).
+ * Column-major.  With binary != 0, omegaBin comes from getBinaryPosition's
+ * circular orbit (massBin, aBin, mass_star) and each statement takes its
+ * BINARY term after the DELT term, as the reference's single statements
+ * evaluate left to right. */
+void ora_source_binary(int jmax, int kmax, int lmax, int j2p, int k2p, int jmin, double delt, double dr, double dz,
+                       double dtheta, const double *r, const double *rho, const double *phi, const double *omega,
+                       const double *p, double *s, double *t, double *a, int binary, double mass_star,
+                       double mass_bin, double a_bin, const double *rhf, const double *u)
 {
     const double quarter = 0.25, half = 0.5, two = 2.0;
     const size_t j2 = (size_t)jmax + 2, k2 = (size_t)kmax + 2;
 #define H_(x, j, k, l) (x)[((size_t)(j) - 1) + j2 * (((size_t)(k) - 1) + k2 * ((size_t)(l) - 1))]
 #define P_(x, j, k, l) (x)[((size_t)(j) - 1) + (size_t)j2p * (((size_t)(k) - 1) + (size_t)k2p * ((size_t)(l) - 1))]
     const int jstart = jmin > 2 ? jmin : 2;   /* radhydro/source.f:33-37 */
+    /* getBinaryPosition's circular orbit (radhydro/ExternalRoutines.f:101-102) */
+    double omega_bin = 0.0;
+    if (binary) {
+        const double mu = mass_bin + mass_star;
+        omega_bin = sqrt((mu) / (a_bin * a_bin * a_bin));
+    }
     for (int l = 1; l <= lmax; l++) {
         int lm = l - 1, lp = l + 1;
         if (l == 1) lm = lmax;
@@ -2199,17 +2211,32 @@ void ora_source(int jmax, int kmax, int lmax, int j2p, int k2p, int jmin, double
                             (P_(rho, j, k, l) + P_(rho, j - 1, k, l)) * (P_(phi, j, k, l) - P_(phi, j - 1, k, l)) /
                                 (two * dr) -
                             (H_(p, j, k, l) - H_(p, j - 1, k, l)) / dr);
+                if (binary) /* source.f:61-62 */
+                    H_(s, j, k, l) = H_(s, j, k, l) +
+                        omega_bin * H_(omega, j, k, l) * rhf[j - 1] * two * P_(rho, j, k, l) * delt;
             }
             for (int j = jstart; j <= jmax + 1; j++)
                 H_(t, j, k, l) = H_(t, j, k, l) -
                     delt * (half * (P_(rho, j, k, l) + P_(rho, j, k - 1, l)) * (P_(phi, j, k, l) - P_(phi, j, k - 1, l)) / dz +
                             (H_(p, j, k, l) - H_(p, j, k - 1, l)) / dz);
-            for (int j = jstart; j <= jmax + 1; j++)
+            for (int j = jstart; j <= jmax + 1; j++) {
                 H_(a, j, k, l) = H_(a, j, k, l) -
                     delt * (P_(rho, j, k, l) * (P_(phi, j, k, lp) - P_(phi, j, k, lm)) + H_(p, j, k, lp) - H_(p, j, k, lm)) /
                         (two * dtheta);
+                if (binary) /* source.f:76-77 */
+                    H_(a, j, k, l) = H_(a, j, k, l) -
+                        P_(rho, j, k, l) * omega_bin * (H_(u, j + 1, k, l) + H_(u, j, k, l)) * delt * rhf[j - 1];
+            }
         }
     }
 #undef H_
 #undef P_
+}
+
+void ora_source(int jmax, int kmax, int lmax, int j2p, int k2p, int jmin, double delt, double dr, double dz,
+                double dtheta, const double *r, const double *rho, const double *phi, const double *omega,
+                const double *p, double *s, double *t, double *a)
+{
+    ora_source_binary(jmax, kmax, lmax, j2p, k2p, jmin, delt, dr, dz, dtheta, r, rho, phi, omega, p, s, t, a, 0, 0.0,
+                      0.0, 0.0, NULL, NULL);
 }

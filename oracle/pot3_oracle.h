@@ -83,6 +83,14 @@ void ora_external_pot_binary(ora_ctx *c, double mass_star, double tmassacc, doub
 void ora_source(int jmax, int kmax, int lmax, int j2p, int k2p, int jmin, double delt, double dr, double dz,
                 double dtheta, const double *r, const double *rho, const double *phi, const double *omega,
                 const double *p, double *s, double *t, double *a);
+/* The same with the BINARY build's terms when binary != 0 (source.f:38-40,
+ * 61-62, 76-77): omegaBin = sqrt((mass_bin + mass_star)/a_bin**3),
+ * S += omegaBin*OMEGA*RHF*2*RHO*DELT, A -= RHO*omegaBin*(U(J+1)+U(J))*DELT*RHF;
+ * u is U(jmax+2, kmax+2, lmax), rhf is RHF(j2p). */
+void ora_source_binary(int jmax, int kmax, int lmax, int j2p, int k2p, int jmin, double delt, double dr, double dz,
+                       double dtheta, const double *r, const double *rho, const double *phi, const double *omega,
+                       const double *p, double *s, double *t, double *a, int binary, double mass_star,
+                       double mass_bin, double a_bin, const double *rhf, const double *u);
 
 /* Low-level routines, exported for unit tests. Arrays are 0-based views of the
  * Fortran 1-based arrays. */

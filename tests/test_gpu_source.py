@@ -1,5 +1,6 @@
 """SOURCE's potential, pressure and rotation terms (radhydro/source.f:45-81)
-on the GPU through the C ABI (chy_source), against the oracle's restatement.
+on the GPU through the C ABI (chy_source, and chy_source_binary for a BINARY
+build), against the oracle's restatement.
 
 Every cell is computed independently with each operation rounded as the
 reference rounds it, so S, T and A must equal the oracle's bit for bit: for
@@ -24,20 +25,23 @@ def fields(jh, kh, seed):
     return dict(omega=f(hs, 2.0, -1.0), p=f(hs, 1e-3), s=f(hs, 1.0, -0.5), t=f(hs, 1.0, -0.5), a=f(hs, 1.0, -0.5))
 
 
-def run_both(chylib, plan, rho, phi, hyd, delt, jmin):
-    """chy_source on the GPU and the oracle on the same arrays; the plan's
-    spacings and R(J) = (J-2) ROF3N."""
+def run_both(chylib, plan, rho, phi, hyd, delt, jmin, binary=None):
+    """chy_source (chy_source_binary with `binary`) on the GPU and the oracle
+    on the same arrays; the plan's spacings, R(J) = (J-2) ROF3N and
+    RHF(J) = R(J) + ROF3N/2."""
     from oracle import oracle as O
     d = {k: chylib.to_cuda_fortran(v) for k, v in hyd.items()}
+    gbin = None if binary is None else dict(binary, u=chylib.to_cuda_fortran(binary["u"]))
     plan.source(chylib.to_cuda_fortran(rho), chylib.to_cuda_fortran(phi), d["omega"], d["p"], d["s"], d["t"],
-                d["a"], delt, jmin=jmin)
+                d["a"], delt, jmin=jmin, binary=gbin)
     import torch
     torch.cuda.synchronize()
     ref = {k: v.copy(order="F") for k, v in hyd.items()}
     g = plan.grid
     r = np.array([(j - 2) * g.rof3n for j in range(1, J + 3)])
+    obin = None if binary is None else dict(binary, rhf=r + g.rof3n / 2.0)
     O.source(r, rho, phi, ref["omega"], ref["p"], ref["s"], ref["t"], ref["a"], delt, g.rof3n, g.zof3n,
-             2.0 * 3.1415926535897932 / L, jmin=jmin)
+             2.0 * 3.1415926535897932 / L, jmin=jmin, binary=obin)
     return {k: d[k].cpu().numpy() for k in ("s", "t", "a")}, ref
 
 
@@ -61,6 +65,29 @@ def test_source_bitwise(chylib, jh, kh, jmin, spacing):
         # cells outside the loops keep their values
         assert np.array_equal(got["t"][:, 0, :], hyd["t"][:, 0, :])
         assert np.array_equal(got["a"][:, kh + 1, :], hyd["a"][:, kh + 1, :])
+
+
+@pytest.mark.parametrize("jh,kh", [(J, K), (48, 24)])
+@pytest.mark.parametrize("jmin", [1, 2, 5])
+def test_source_binary_bitwise(chylib, jh, kh, jmin):
+    """The BINARY build's terms (radhydro/source.f:61-62, 76-77) with
+    getBinaryPosition's OMEGABIN: S and A bitwise the oracle's, T as in a
+    BINARY = 0 build, and S, A differing from the BINARY = 0 results."""
+    plan = chylib.Plan(chylib.grid(J, K, L), "fp64", 1)
+    rng = np.random.default_rng(13)
+    rho = np.asfortranarray(rng.random((J + 2, K + 2, L)))
+    phi = np.asfortranarray(-1.0 - rng.random((J + 2, K + 2, L)))
+    hyd = fields(jh, kh, 7)
+    u = np.asfortranarray(rng.random(hyd["omega"].shape) - 0.5)
+    # a close companion, so that its terms are visible in S and A
+    binary = dict(u=u, mass_star=1.0, mass_bin=0.5, a_bin=1.5)
+    got, ref = run_both(chylib, plan, rho, phi, hyd, 3.7e-4, jmin, binary=binary)
+    for k in ("s", "t", "a"):
+        assert np.array_equal(got[k], ref[k]), k
+    plain, _ = run_both(chylib, plan, rho, phi, hyd, 3.7e-4, jmin)
+    assert np.array_equal(got["t"], plain["t"])
+    for k in ("s", "a"):
+        assert not np.array_equal(got[k], plain[k]), k
 
 
 def test_source_after_solve_and_external_potential(chylib):
@@ -91,4 +118,7 @@ def test_source_argument_checks(chylib):
     assert e.value.status == 11   # CHY_ERR_DIMS: hydro grid larger than the plan's
     with pytest.raises(chylib.ChyError):
         plan.source(x, x, x, x, x, x, x, 1e-3, jmin=0)
+    with pytest.raises(chylib.ChyError) as e:
+        plan.source(x, x, x, x, x, x, x, 1e-3, binary=dict(u=x, mass_star=1.0, a_bin=0.0))
+    assert e.value.status == 10   # CHY_ERR_ARG: the separation must be positive
     torch.cuda.synchronize()

@@ -236,6 +236,8 @@ def test_external_and_source_argument_checks(chylib):
     assert C.sizeof(chylib.ChyBinary) == 2 * 8
     b = chylib.ChyBinary(1.0, 100.0)
     assert L.chy_plan_set_binary(None, C.byref(b)) == 10
+    assert L.chy_source_binary(None, C.byref(a), C.byref(b), 1.0, None, None) == 10
+    assert L.chy_source_binary(None, C.byref(a), None, 1.0, None, None) == 10
     assert C.sizeof(chylib.ChyTune) == 6 * 4 + 2 * 8 + 8
     # argument errors come with their own message
     o = chylib.ServerOpts()

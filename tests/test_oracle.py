@@ -393,3 +393,34 @@ def test_source_terms_match_numpy_and_conserve(ora):
     # untouched: J = 1 and 2 of S, K = 1 and KMAX+2 everywhere
     assert np.array_equal(s[:2], s0[:2]) and np.array_equal(t[:, 0], t0[:, 0])
     assert np.array_equal(a[:, K + 1], a0[:, K + 1])
+
+
+def test_source_binary_terms_match_numpy(ora):
+    """The BINARY build's terms (radhydro/source.f:61-62, 76-77): the oracle's
+    S and A against numpy statements of the same left-to-right products,
+    added after the BINARY = 0 update of the same statement; T unchanged."""
+    import math
+    J, K, L = 12, 6, 8
+    rng = np.random.default_rng(6)
+    hs = (J + 2, K + 2, L)
+    rho, phi, omega, p, u = (np.asfortranarray(rng.random(hs)) for _ in range(5))
+    s, t, a = (np.asfortranarray(rng.random(hs)) for _ in range(3))
+    r = (np.arange(1, J + 3) - 2) * 0.1
+    rhf = r + 0.05
+    dr, dz, dth, delt = 0.1, 0.05, 2 * np.pi / L, 1e-3
+    plain = [x.copy(order="F") for x in (s, t, a)]
+    ora.source(r, rho, phi, omega, p, *plain, delt, dr, dz, dth, jmin=3)
+    ora.source(r, rho, phi, omega, p, s, t, a, delt, dr, dz, dth, jmin=3,
+               binary=dict(mass_star=1.0, mass_bin=0.5, a_bin=1.5, rhf=rhf, u=u))
+    mu = 0.5 + 1.0
+    ob = math.sqrt(mu / (1.5 * 1.5 * 1.5))      # getBinaryPosition (ExternalRoutines.f:101-102)
+    k = slice(1, K + 1)
+    j = slice(3, J + 1)          # S: J = JSTART+1..JMAX1 with JSTART = 3
+    want_s = plain[0][j, k] + ob * omega[j, k] * rhf[j, None, None] * 2.0 * rho[j, k] * delt
+    assert np.array_equal(s[j, k], want_s)
+    jj = slice(2, J + 1)         # A: J = JSTART..JMAX1
+    want_a = plain[2][jj, k] - rho[jj, k] * ob * (u[3:J + 2, k] + u[jj, k]) * delt * rhf[jj, None, None]
+    assert np.array_equal(a[jj, k], want_a)
+    assert np.array_equal(t, plain[1])
+    # cells outside the loops are the BINARY = 0 build's
+    assert np.array_equal(s[:3], plain[0][:3]) and np.array_equal(a[:2], plain[2][:2])
